@@ -1,0 +1,178 @@
+/*
+ * morphoshell_gpu.h -- C ABI of the B200 force-and-dynamics loop.
+ *
+ * Drop-in replacement for the per-step functions that MorphoShell's main
+ * loop (source_files/main.cpp:269-508) calls with caller-owned Eigen
+ * objects.  Here the library owns device memory; host arrays are copied in
+ * and out and no host pointer is retained after a call returns.  All arrays
+ * are plain C arrays:
+ *
+ *   dofs, velocities, forces : SoA, [X(N) | Y(N) | Z(N)]      (main.cpp:235-237)
+ *   continuum quantities     : 15 per triangle, ordered
+ *                              Xx Xy Xxx Xxy Xyy  Yx Yy Yxx Yxy Yyy  Zx Zy Zxx Zxy Zyy
+ *                                                               (calc_deriv_mats.cpp:60-61)
+ *   a, b, abar, bbar, normals: 3 per triangle (xx, xy, yy) / (x, y, z), row-major
+ *
+ * Every function returns an ms_status; 0 is success.  One handle belongs to
+ * one host thread and one CUDA stream; calls on a handle are not re-entrant.
+ * Floating-point work is IEEE double unless the handle was created with
+ * MS_PRECISION_MIXED.
+ */
+#ifndef MORPHOSHELL_GPU_H
+#define MORPHOSHELL_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum ms_status {
+    MS_OK = 0,
+    MS_ERR_INVALID_ARGUMENT = 1,
+    MS_ERR_CUDA = 2,
+    MS_ERR_IMPLAUSIBLE_FORCE = 3, /* advance_dynamics.cpp:58-73 ("implausibly_high_force") */
+    MS_ERR_NON_FINITE = 4,
+    MS_ERR_TIMEOUT = 5,
+    MS_ERR_NO_DEVICE = 6,
+    MS_ERR_OUT_OF_MEMORY = 7,
+    MS_ERR_UNSUPPORTED = 8
+} ms_status;
+
+typedef enum ms_precision {
+    MS_PRECISION_FP64 = 0,  /* all per-step arithmetic in double */
+    MS_PRECISION_MIXED = 1  /* per-triangle arithmetic and gathers in float; node state, metric
+                               inverse and reductions in double */
+} ms_precision;
+
+/* Mesh tables produced by the host set-up (read_vtk_data, calc_mesh_info,
+ * set_up_patch_fitting, calc_deriv_mats, calc_dof_masses).  Triangle t's
+ * patch is patch_ids[6t..6t+5]: its three vertices (Tri_Class::vertex_ids)
+ * then the three extra patch nodes (Tri_Class::non_vertex_patch_nodes_ids).
+ * deriv_coeffs[24t..24t+23] holds the non-zeros of triangle t's 15 rows of
+ * the sparse matrix built by calc_deriv_mats.cpp:46-136: d/dx weights of the
+ * three vertices, d/dy weights of the three vertices, then for each patch
+ * node n = 0..5 its (xx, xy, yy) second-derivative weights. */
+typedef struct ms_mesh_desc {
+    int32_t num_nodes;
+    int32_t num_tris;
+    const int32_t* patch_ids;         /* 6 * num_tris */
+    const double* deriv_coeffs;       /* 24 * num_tris */
+    const double* ref_area;           /* num_tris  (Tri_Class::ref_area) */
+    const double* ref_thickness;      /* num_tris  (Tri_Class::ref_thickness) */
+    const double* ref_shear_modulus;  /* num_tris  (Tri_Class::ref_shear_modulus) */
+    const double* node_mass;          /* num_nodes (dof mass, equal for x, y, z; calc_dof_masses.cpp:50-58) */
+    const uint8_t* is_constrained;    /* num_nodes (Node_Class::is_constrained) */
+    const uint8_t* is_boundary;       /* num_nodes (Node_Class::is_boundary); may be NULL, used only by
+                                         the angle deficits of ms_output_quantities */
+} ms_mesh_desc;
+
+/* Scalars of Stuff_Class that the per-step functions read. */
+typedef struct ms_params {
+    double def_poisson_ratio;
+    double bend_stiffening_scale_factor;
+    double ref_density;
+    double min_ref_thickness;
+    double char_force_scale;
+    double char_speed_scale;
+    double force_to_char_force_ratio_equil_threshold;
+    double speed_to_char_speed_ratio_equil_threshold;
+} ms_params;
+
+/* Result of is_at_equilibrium (is_at_equilibrium.cpp:51-99). */
+typedef struct ms_equil_result {
+    double max_force;      /* max over nodes of |F_n| */
+    double max_speed;      /* max over nodes of |v_n| */
+    int64_t max_force_node;/* first node attaining it */
+    int64_t max_speed_node;
+    int32_t at_equilibrium;
+} ms_equil_result;
+
+/* What the fused stepper did (ms_step_n). */
+typedef struct ms_step_report {
+    int32_t steps_done;          /* steps fully advanced */
+    int32_t error_step;          /* index of the step that failed, or -1 */
+    int64_t offending_dof;       /* first dof failing the force guard, or -1 */
+    double offending_force;
+    ms_equil_result equil;       /* filled when the last step carried an equilibrium check */
+} ms_step_report;
+
+typedef struct ms_handle ms_handle;
+
+/* ---- lifetime ------------------------------------------------------- */
+/* Uploads the mesh tables; initial dofs and velocities are zero.  device < 0
+ * selects the current device.  Replaces the allocations of main.cpp:240-260. */
+ms_status ms_create(const ms_mesh_desc* mesh, const ms_params* params, int device, int precision,
+                    ms_handle** out);
+ms_status ms_destroy(ms_handle* h);
+const char* ms_last_error(const ms_handle* h);
+const char* ms_status_string(int status);
+
+/* ---- state transfer (move_nodes_to_ansatz_positions.cpp:31-38, output) --- */
+ms_status ms_upload_dofs(ms_handle* h, const double* dofs /*3N*/, const double* velocities /*3N or NULL = zeros*/);
+ms_status ms_download_dofs(ms_handle* h, double* dofs /*3N or NULL*/, double* velocities /*3N or NULL*/);
+ms_status ms_download_forces(ms_handle* h, double* forces /*3N*/);
+
+/* ---- programmed tensors and dialling (do_dialling.cpp:36-260) ---------- */
+/* abar_info is num_tris x ka, bbar_info num_tris x kb (row-major, the
+ * CELL_DATA fields of the input file).  protocol selects the dialling
+ * protocol of do_dialling.cpp (1: linear abar/bbar, 2: bbar then abar,
+ * 3: LCE lambda, 4: piecewise lambda checkpoints, 5: isotropic swelling). */
+ms_status ms_set_programmed(ms_handle* h, int protocol, const double* abar_info, int ka, const double* bbar_info,
+                            int kb, double dial_factors_to_hold_at_spacing, int dialling_from_ansatz);
+/* a and b at zero dial factor (main.cpp:213-219 and :320-329); NULL keeps
+ * the flat reference state a = I, b = 0. */
+ms_status ms_set_zero_dial_state(ms_handle* h, const double* a0 /*3T or NULL*/, const double* b0 /*3T or NULL*/);
+/* do_dialling: sets abar, bbar (thickness and modulus stay at reference). */
+ms_status ms_do_dialling(ms_handle* h, double dial_factor);
+ms_status ms_download_programmed(ms_handle* h, double* abar /*3T*/, double* bbar /*3T*/);
+
+/* ---- the reference's per-step sequence, one call each ------------------ */
+/* calc_surface_derivs.cpp:27-34: cq = D * dofs.  cq may be NULL (kept on device). */
+ms_status ms_surface_derivs(ms_handle* h, double* cq /*15T or NULL*/);
+/* calc_a_comps_and_b_comps_and_normals.cpp:27-62, from the last cq. */
+ms_status ms_a_b_normals(ms_handle* h, double* a /*3T*/, double* b /*3T*/, double* normals /*3T*/);
+/* calc_deformation_forces.cpp:40-185, from the last cq: dE/dcq per triangle
+ * and forces = -D^T dE/dcq.  Either output may be NULL. */
+ms_status ms_deformation_forces(ms_handle* h, double* forces /*3N or NULL*/, double* del_energy_by_del_cq /*15T or NULL*/);
+/* calc_non_deformation_forces.cpp:37-57 (damping; no glass slides). */
+ms_status ms_non_deformation_forces(ms_handle* h, double damping_factor, int using_gradient_descent);
+/* impose_constraints.cpp:48-69 */
+ms_status ms_impose_constraints(ms_handle* h);
+/* is_at_equilibrium.cpp:51-99 */
+ms_status ms_is_at_equilibrium(ms_handle* h, ms_equil_result* out);
+/* advance_dynamics.cpp:47-93: force guard, then v += dt F / m, x += dt v.
+ * Returns MS_ERR_IMPLAUSIBLE_FORCE (state untouched) if the guard trips. */
+ms_status ms_advance_dynamics(ms_handle* h, double timestep, double damping_factor, int using_gradient_descent,
+                              int64_t* offending_dof, double* offending_force);
+
+/* ---- fused stepper: the whole main.cpp:308-488 body per step ----------
+ * Runs n steps of: surface derivs -> (dialling) -> deformation forces ->
+ * damping -> constraints -> (equilibrium check on the last step if
+ * check_last) -> force guard -> symplectic Euler, as two kernels per step
+ * captured in a CUDA graph.  dial_factors[i] (length n, may be NULL when
+ * dialling == 0) is the dial factor step i dials to.  Stops at the first
+ * step whose force guard trips and reports it; the state is then the state
+ * before that step, as in main.cpp:448-474. */
+ms_status ms_step_n(ms_handle* h, int n, const double* dial_factors, int dialling, double timestep,
+                    double damping_factor, int using_gradient_descent, int check_last, ms_step_report* report);
+
+/* ---- output diagnostics (main.cpp:412-436) ------------------------------
+ * From the current dofs (recomputes cq).  Any output may be NULL.
+ * curvatures T x 2 (Gauss, mean; calc_curvatures.cpp), energy_densities
+ * T x 2 (stretch, bend; calc_energy_densities.cpp), strains T
+ * (calc_strains.cpp), stresses T x 8 (calc_stresses.cpp), angle_deficits N
+ * (calc_angle_deficits.cpp), energies[3] = stretch, bend, kinetic
+ * (calc_energies.cpp). */
+ms_status ms_output_quantities(ms_handle* h, double* curvatures, double* energy_densities, double* strains,
+                               double* stresses, double* angle_deficits, double* energies);
+
+/* Library and device description, for logs. */
+ms_status ms_device_info(char* buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MORPHOSHELL_GPU_H */

@@ -1,0 +1,345 @@
+"""B200-native force-and-dynamics loop of MorphoShell.
+
+Python access to the native library ``lib/libmorphoshell.so`` (host set-up
+plus sm_100a kernels) through its C ABI (``include/morphoshell_gpu.h`` and
+``include/morphoshell_host.h``).  There is no Python or CPU implementation of
+the per-step physics here: if the library is missing or no GPU is present,
+the GPU calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libmorphoshell.so")
+
+MS_OK = 0
+MS_ERR_IMPLAUSIBLE_FORCE = 3
+MS_PRECISION_FP64 = 0
+MS_PRECISION_MIXED = 1
+
+GPU_SYMBOLS = [
+    "ms_create", "ms_destroy", "ms_last_error", "ms_status_string", "ms_upload_dofs", "ms_download_dofs",
+    "ms_download_forces", "ms_set_programmed", "ms_set_zero_dial_state", "ms_do_dialling",
+    "ms_download_programmed", "ms_surface_derivs", "ms_a_b_normals", "ms_deformation_forces",
+    "ms_non_deformation_forces", "ms_impose_constraints", "ms_is_at_equilibrium", "ms_advance_dynamics",
+    "ms_step_n", "ms_output_quantities", "ms_device_info",
+]
+HOST_SYMBOLS = [
+    "msh_load", "msh_free", "msh_last_error", "msh_get_scalars", "msh_get_desc", "msh_get_dofs",
+    "msh_get_programmed", "msh_get_tri_vertices", "msh_get_boundary", "msh_run",
+]
+
+
+class MsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class ms_mesh_desc(C.Structure):
+    _fields_ = [("num_nodes", C.c_int32), ("num_tris", C.c_int32), ("patch_ids", C.POINTER(C.c_int32)),
+                ("deriv_coeffs", C.POINTER(C.c_double)), ("ref_area", C.POINTER(C.c_double)),
+                ("ref_thickness", C.POINTER(C.c_double)), ("ref_shear_modulus", C.POINTER(C.c_double)),
+                ("node_mass", C.POINTER(C.c_double)), ("is_constrained", C.POINTER(C.c_uint8)),
+                ("is_boundary", C.POINTER(C.c_uint8))]
+
+
+class ms_params(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "def_poisson_ratio", "bend_stiffening_scale_factor", "ref_density", "min_ref_thickness",
+        "char_force_scale", "char_speed_scale", "force_to_char_force_ratio_equil_threshold",
+        "speed_to_char_speed_ratio_equil_threshold")]
+
+
+class ms_equil_result(C.Structure):
+    _fields_ = [("max_force", C.c_double), ("max_speed", C.c_double), ("max_force_node", C.c_int64),
+                ("max_speed_node", C.c_int64), ("at_equilibrium", C.c_int32)]
+
+
+class ms_step_report(C.Structure):
+    _fields_ = [("steps_done", C.c_int32), ("error_step", C.c_int32), ("offending_dof", C.c_int64),
+                ("offending_force", C.c_double), ("equil", ms_equil_result)]
+
+
+class msh_scalars(C.Structure):
+    _fields_ = ([(n, C.c_int32) for n in ("num_nodes", "num_tris", "num_edges", "num_boundary_nodes",
+                                          "num_boundary_edges", "dialling_protocol", "dialling_from_ansatz",
+                                          "using_gradient_descent_dynamics", "num_gd_steps", "output_regularly")]
+                + [(n, C.c_int64) for n in ("steps_between_outputs", "timesteps_per_dial_phase",
+                                            "timesteps_between_equil_checks")]
+                + [(n, C.c_double) for n in (
+                    "sample_char_length", "approx_min_tri_size", "min_ref_thickness", "min_ref_shear_modulus",
+                    "char_long_time", "dial_phase_time", "timestep", "damping_factor_1", "damping_factor_2",
+                    "char_force_scale", "char_speed_scale", "char_stretch_energy_density_scale", "total_ref_area",
+                    "dial_factors_to_hold_at_spacing", "dial_factor_to_start_from", "def_poisson_ratio",
+                    "bend_stiffening_scale_factor", "ref_density", "force_thresh", "speed_thresh")])
+
+
+class msh_run_options(C.Structure):
+    _fields_ = [("max_steps", C.c_int64), ("stop_at_final_equilibrium", C.c_int32), ("write_outputs", C.c_int32),
+                ("precision", C.c_int32), ("device", C.c_int32), ("quiet", C.c_int32), ("output_dir", C.c_char_p)]
+
+
+class msh_run_result(C.Structure):
+    _fields_ = [("status", C.c_int32), ("steps", C.c_int64), ("final_dial_factor", C.c_double),
+                ("sim_time", C.c_double), ("equilibria_reached", C.c_int32), ("final_status", C.c_int32),
+                ("wall_seconds", C.c_double), ("last_max_force_ratio", C.c_double),
+                ("last_max_speed_ratio", C.c_double)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """The loaded native library (built in-tree by ``morphoshell_b200.build``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError("native library %s is missing; run `python -m morphoshell_b200.build`" % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        d = C.POINTER(C.c_double)
+        L.ms_create.argtypes = [P(ms_mesh_desc), P(ms_params), C.c_int, C.c_int, P(C.c_void_p)]
+        L.ms_destroy.argtypes = [C.c_void_p]
+        L.ms_last_error.argtypes = [C.c_void_p]
+        L.ms_last_error.restype = C.c_char_p
+        L.ms_status_string.argtypes = [C.c_int]
+        L.ms_status_string.restype = C.c_char_p
+        L.ms_upload_dofs.argtypes = [C.c_void_p, d, d]
+        L.ms_download_dofs.argtypes = [C.c_void_p, d, d]
+        L.ms_download_forces.argtypes = [C.c_void_p, d]
+        L.ms_set_programmed.argtypes = [C.c_void_p, C.c_int, d, C.c_int, d, C.c_int, C.c_double, C.c_int]
+        L.ms_set_zero_dial_state.argtypes = [C.c_void_p, d, d]
+        L.ms_do_dialling.argtypes = [C.c_void_p, C.c_double]
+        L.ms_download_programmed.argtypes = [C.c_void_p, d, d]
+        L.ms_surface_derivs.argtypes = [C.c_void_p, d]
+        L.ms_a_b_normals.argtypes = [C.c_void_p, d, d, d]
+        L.ms_deformation_forces.argtypes = [C.c_void_p, d, d]
+        L.ms_non_deformation_forces.argtypes = [C.c_void_p, C.c_double, C.c_int]
+        L.ms_impose_constraints.argtypes = [C.c_void_p]
+        L.ms_is_at_equilibrium.argtypes = [C.c_void_p, P(ms_equil_result)]
+        L.ms_advance_dynamics.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, P(C.c_int64), d]
+        L.ms_step_n.argtypes = [C.c_void_p, C.c_int, d, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
+                                P(ms_step_report)]
+        L.ms_output_quantities.argtypes = [C.c_void_p, d, d, d, d, d, d]
+        L.ms_device_info.argtypes = [C.c_char_p, C.c_size_t]
+        L.msh_load.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, P(C.c_void_p)]
+        L.msh_free.argtypes = [C.c_void_p]
+        L.msh_free.restype = None
+        L.msh_last_error.restype = C.c_char_p
+        L.msh_get_scalars.argtypes = [C.c_void_p, P(msh_scalars)]
+        L.msh_get_desc.argtypes = [C.c_void_p, P(ms_mesh_desc), P(ms_params)]
+        L.msh_get_dofs.argtypes = [C.c_void_p, C.c_int, d]
+        L.msh_get_programmed.argtypes = [C.c_void_p, d, P(C.c_int32), d, P(C.c_int32)]
+        L.msh_get_tri_vertices.argtypes = [C.c_void_p, P(C.c_int32)]
+        L.msh_get_boundary.argtypes = [C.c_void_p, P(C.c_uint8)]
+        L.msh_run.argtypes = [C.c_void_p, P(msh_run_options), P(msh_run_result), d]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Model:
+    """Host set-up of one run (msh_load): settings + mesh (+ ansatz)."""
+
+    def __init__(self, settings_path: str, vtk_path: str, ansatz_path: str | None = None,
+                 quiet: bool = True, noise: bool = True):
+        L = lib()
+        h = C.c_void_p()
+        flags = (1 if quiet else 0) | (0 if noise else 2)
+        rc = L.msh_load(settings_path.encode(), vtk_path.encode(),
+                        ansatz_path.encode() if ansatz_path else None, flags, C.byref(h))
+        if rc != 0:
+            raise RuntimeError(L.msh_last_error().decode())
+        self._h = h
+        s = msh_scalars()
+        L.msh_get_scalars(h, C.byref(s))
+        self.scalars = s
+        self.desc = ms_mesh_desc()
+        self.params = ms_params()
+        L.msh_get_desc(h, C.byref(self.desc), C.byref(self.params))
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().msh_free(self._h)
+            self._h = None
+
+    @property
+    def num_nodes(self) -> int:
+        return self.scalars.num_nodes
+
+    @property
+    def num_tris(self) -> int:
+        return self.scalars.num_tris
+
+    def dofs(self, which: int = 1) -> np.ndarray:
+        out = np.empty(3 * self.num_nodes)
+        lib().msh_get_dofs(self._h, which, _dp(out))
+        return out
+
+    def programmed(self):
+        ka, kb = C.c_int32(), C.c_int32()
+        lib().msh_get_programmed(self._h, None, C.byref(ka), None, C.byref(kb))
+        a = np.empty((self.num_tris, ka.value))
+        b = np.empty((self.num_tris, kb.value))
+        lib().msh_get_programmed(self._h, _dp(a), None, _dp(b), None)
+        return a, b
+
+    def tables(self) -> dict:
+        """numpy copies of the mesh tables handed to ms_create."""
+        d, T, N = self.desc, self.num_tris, self.num_nodes
+        np_ = np.ctypeslib.as_array
+        return {
+            "patch_ids": np_(d.patch_ids, (T * 6,)).reshape(T, 6).copy(),
+            "deriv_coeffs": np_(d.deriv_coeffs, (T * 24,)).reshape(T, 24).copy(),
+            "ref_area": np_(d.ref_area, (T,)).copy(),
+            "ref_thickness": np_(d.ref_thickness, (T,)).copy(),
+            "ref_shear_modulus": np_(d.ref_shear_modulus, (T,)).copy(),
+            "node_mass": np_(d.node_mass, (N,)).copy(),
+            "is_constrained": np_(d.is_constrained, (N,)).copy(),
+            "is_boundary": np_(d.is_boundary, (N,)).copy(),
+        }
+
+    def run(self, max_steps: int = 0, precision: int = MS_PRECISION_FP64, output_dir: str | None = None,
+            stop_at_final_equilibrium: bool = True, quiet: bool = True, device: int = -1):
+        o = msh_run_options(max_steps, int(stop_at_final_equilibrium), 1 if output_dir else 0, precision, device,
+                            int(quiet), output_dir.encode() if output_dir else None)
+        r = msh_run_result()
+        out = np.empty(3 * self.num_nodes)
+        rc = lib().msh_run(self._h, C.byref(o), C.byref(r), _dp(out))
+        if rc != 0 and r.status != MS_ERR_IMPLAUSIBLE_FORCE:
+            raise RuntimeError(lib().msh_last_error().decode())
+        return r, out
+
+
+class GpuLoop:
+    """One device handle (ms_create) over a Model's tables."""
+
+    def __init__(self, model: Model, precision: int = MS_PRECISION_FP64, device: int = -1):
+        L = lib()
+        h = C.c_void_p()
+        rc = L.ms_create(C.byref(model.desc), C.byref(model.params), device, precision, C.byref(h))
+        if rc != MS_OK:
+            raise MsError(rc, "ms_create: %s" % L.ms_status_string(rc).decode())
+        self._h = h
+        self.N = model.num_nodes
+        self.T = model.num_tris
+        self.model = model
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ms_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def _chk(self, rc, what):
+        if rc != MS_OK:
+            raise MsError(rc, "%s: %s (%s)" % (what, lib().ms_status_string(rc).decode(),
+                                                lib().ms_last_error(self._h).decode()))
+
+    def upload(self, dofs, vel=None):
+        self._chk(lib().ms_upload_dofs(self._h, _dp(_f64(dofs)), _dp(None if vel is None else _f64(vel))), "upload")
+
+    def download(self):
+        x = np.empty(3 * self.N)
+        v = np.empty(3 * self.N)
+        self._chk(lib().ms_download_dofs(self._h, _dp(x), _dp(v)), "download")
+        return x, v
+
+    def forces(self):
+        f = np.empty(3 * self.N)
+        self._chk(lib().ms_download_forces(self._h, _dp(f)), "forces")
+        return f
+
+    def set_programmed(self, protocol, abar_info, bbar_info, spacing, from_ansatz=False):
+        a, b = _f64(abar_info), _f64(bbar_info)
+        self._a, self._b = a, b
+        self._chk(lib().ms_set_programmed(self._h, protocol, _dp(a), a.shape[1], _dp(b), b.shape[1], spacing,
+                                          int(from_ansatz)), "set_programmed")
+
+    def set_zero_dial_state(self, a0=None, b0=None):
+        self._chk(lib().ms_set_zero_dial_state(self._h, _dp(None if a0 is None else _f64(a0)),
+                                               _dp(None if b0 is None else _f64(b0))), "set_zero_dial_state")
+
+    def do_dialling(self, dial):
+        self._chk(lib().ms_do_dialling(self._h, dial), "do_dialling")
+
+    def programmed(self):
+        a = np.empty((self.T, 3))
+        b = np.empty((self.T, 3))
+        self._chk(lib().ms_download_programmed(self._h, _dp(a), _dp(b)), "download_programmed")
+        return a, b
+
+    def surface_derivs(self):
+        cq = np.empty(15 * self.T)
+        self._chk(lib().ms_surface_derivs(self._h, _dp(cq)), "surface_derivs")
+        return cq
+
+    def a_b_normals(self):
+        a, b, n = (np.empty((self.T, 3)) for _ in range(3))
+        self._chk(lib().ms_a_b_normals(self._h, _dp(a), _dp(b), _dp(n)), "a_b_normals")
+        return a, b, n
+
+    def deformation_forces(self):
+        f = np.empty(3 * self.N)
+        de = np.empty(15 * self.T)
+        self._chk(lib().ms_deformation_forces(self._h, _dp(f), _dp(de)), "deformation_forces")
+        return f, de
+
+    def non_deformation_forces(self, damping, gd=False):
+        self._chk(lib().ms_non_deformation_forces(self._h, damping, int(gd)), "non_deformation_forces")
+
+    def impose_constraints(self):
+        self._chk(lib().ms_impose_constraints(self._h), "impose_constraints")
+
+    def is_at_equilibrium(self):
+        r = ms_equil_result()
+        self._chk(lib().ms_is_at_equilibrium(self._h, C.byref(r)), "is_at_equilibrium")
+        return r
+
+    def advance_dynamics(self, dt, damping, gd=False):
+        dof = C.c_int64(-1)
+        f = C.c_double(0.0)
+        rc = lib().ms_advance_dynamics(self._h, dt, damping, int(gd), C.byref(dof), C.byref(f))
+        if rc == MS_ERR_IMPLAUSIBLE_FORCE:
+            raise MsError(rc, "implausibly_high_force (dof %d, force %g)" % (dof.value, f.value))
+        self._chk(rc, "advance_dynamics")
+
+    def step_n(self, n, dials=None, dt=0.0, damping=0.0, gd=False, check_last=False):
+        rep = ms_step_report()
+        dl = None if dials is None else _f64(dials)
+        rc = lib().ms_step_n(self._h, n, _dp(dl), 0 if dl is None else 1, dt, damping, int(gd), int(check_last),
+                             C.byref(rep))
+        if rc == MS_ERR_IMPLAUSIBLE_FORCE:
+            err = MsError(rc, "implausibly_high_force at step %d (dof %d)" % (rep.error_step, rep.offending_dof))
+            err.report = rep
+            raise err
+        self._chk(rc, "step_n")
+        return rep
+
+    def output_quantities(self):
+        T, N = self.T, self.N
+        curv, ed = np.empty((T, 2)), np.empty((T, 2))
+        strain, stress, dfc, en = np.empty(T), np.empty((T, 8)), np.empty(N), np.empty(3)
+        self._chk(lib().ms_output_quantities(self._h, _dp(curv), _dp(ed), _dp(strain), _dp(stress), _dp(dfc),
+                                             _dp(en)), "output_quantities")
+        return {"curvatures": curv, "energy_densities": ed, "strains": strain, "stresses": stress,
+                "angle_deficits": dfc, "energies": en}
+
+
+def device_info() -> str:
+    buf = C.create_string_buffer(256)
+    lib().ms_device_info(buf, 256)
+    return buf.value.decode()

@@ -1,0 +1,709 @@
+// C ABI of the force-and-dynamics loop (include/morphoshell_gpu.h): device
+// memory ownership, the one-call-per-reference-function path, the fused
+// stepper captured in CUDA graphs, and the output diagnostics.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../../include/morphoshell_gpu.h"
+#include "internal.cuh"
+
+using namespace msb;
+
+namespace {
+
+// Steps per captured graph chunk (even, so every chunk starts on the same
+// ping-pong buffer).
+constexpr int kChunk = 128;
+
+struct GraphKey {
+    int len, parity, dial_mode, gd, check_last;
+    double dt, damping;
+    bool operator==(const GraphKey& o) const {
+        return len == o.len && parity == o.parity && dial_mode == o.dial_mode && gd == o.gd &&
+               check_last == o.check_last && dt == o.dt && damping == o.damping;
+    }
+};
+
+struct GraphEntry {
+    GraphKey key;
+    cudaGraphExec_t exec;
+    long long last_use;
+};
+
+}  // namespace
+
+struct ms_handle {
+    int device = 0;
+    int precision = 0;
+    cudaStream_t stream = nullptr;
+    DevMesh m{};
+    DevState s{};
+    ms_params params{};
+    double rho_hh = 0, force_limit = 0;
+    int cur = 0;  // buffer holding the current state
+    // dialling
+    int protocol = 1;
+    double spacing = 1.0;
+    int from_ansatz = 0;
+    bool programmed = false;
+    // allocations
+    std::vector<void*> allocs;
+    double* d_dials = nullptr;
+    int dials_cap = 0;
+    double* h_dials = nullptr;  // pinned
+    int h_dials_cap = 0;
+    DevError* h_err = nullptr;  // pinned mirror
+    DevEquil* h_equil = nullptr;
+    double* d_scratch_tri = nullptr;  // [2][T]
+    double* d_scratch_node = nullptr; // [N]
+    double* d_sum_partial = nullptr;  // [512]
+    double* d_sums = nullptr;         // [4]
+    double* d_out = nullptr;          // generic output staging, sized on demand
+    size_t out_cap = 0;
+    std::vector<GraphEntry> graphs;
+    long long use_clock = 0;
+    std::string last_error;
+};
+
+namespace {
+
+ms_status fail(ms_handle* h, ms_status st, const std::string& msg) {
+    if (h) h->last_error = msg;
+    return st;
+}
+
+ms_status cuda_fail(ms_handle* h, cudaError_t e, const char* what) {
+    std::string msg = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return fail(h, MS_ERR_OUT_OF_MEMORY, msg);
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return fail(h, MS_ERR_NO_DEVICE, msg);
+    return fail(h, MS_ERR_CUDA, msg);
+}
+
+#define MS_CUDA(h, call)                                     \
+    do {                                                     \
+        cudaError_t e_ = (call);                             \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, #call); \
+    } while (0)
+
+template <typename T>
+ms_status dalloc(ms_handle* h, T** p, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMalloc");
+    h->allocs.push_back(q);
+    *p = static_cast<T*>(q);
+    return MS_OK;
+}
+
+#define MS_TRY(expr)                   \
+    do {                               \
+        ms_status st_ = (expr);        \
+        if (st_ != MS_OK) return st_;  \
+    } while (0)
+
+void clear_graphs(ms_handle* h) {
+    for (auto& g : h->graphs) cudaGraphExecDestroy(g.exec);
+    h->graphs.clear();
+}
+
+// Transpose a row-major rows x cols host array into [cols][rows] on the device.
+template <typename T>
+ms_status upload_transposed(ms_handle* h, T* dst, const T* src, size_t rows, int cols) {
+    std::vector<T> tmp(rows * cols);
+    for (size_t r = 0; r < rows; ++r)
+        for (int c = 0; c < cols; ++c) tmp[(size_t)c * rows + r] = src[r * cols + c];
+    MS_CUDA(h, cudaMemcpy(dst, tmp.data(), tmp.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return MS_OK;
+}
+
+template <typename T>
+ms_status download_transposed(ms_handle* h, T* dst, const T* src_dev, size_t rows, int cols) {
+    std::vector<T> tmp(rows * cols);
+    MS_CUDA(h, cudaMemcpy(tmp.data(), src_dev, tmp.size() * sizeof(T), cudaMemcpyDeviceToHost));
+    for (size_t r = 0; r < rows; ++r)
+        for (int c = 0; c < cols; ++c) dst[r * cols + c] = tmp[(size_t)c * rows + r];
+    return MS_OK;
+}
+
+ms_status reset_error(ms_handle* h) {
+    DevError z{};
+    z.flag = 0;
+    z.base = 0;
+    z.guard_key = ~0ULL;
+    MS_CUDA(h, cudaMemcpyAsync(h->s.err, &z, sizeof(DevError), cudaMemcpyHostToDevice, h->stream));
+    return MS_OK;
+}
+
+ms_status ensure_out(ms_handle* h, size_t bytes) {
+    if (h->out_cap >= bytes) return MS_OK;
+    if (h->d_out) {
+        cudaFree(h->d_out);
+        h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->d_out), h->allocs.end());
+        h->d_out = nullptr;
+    }
+    MS_TRY(dalloc(h, reinterpret_cast<char**>(&h->d_out), bytes));
+    h->out_cap = bytes;
+    return MS_OK;
+}
+
+bool lce_fusable(const ms_handle* h) { return h->protocol == 3 && !h->from_ansatz && h->precision >= 0; }
+
+}  // namespace
+
+extern "C" {
+
+const char* ms_status_string(int st) {
+    switch (st) {
+        case MS_OK: return "ok";
+        case MS_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case MS_ERR_CUDA: return "CUDA error";
+        case MS_ERR_IMPLAUSIBLE_FORCE: return "implausibly_high_force";
+        case MS_ERR_NON_FINITE: return "non-finite value";
+        case MS_ERR_TIMEOUT: return "timeout";
+        case MS_ERR_NO_DEVICE: return "no CUDA device";
+        case MS_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case MS_ERR_UNSUPPORTED: return "unsupported";
+        default: return "unknown status";
+    }
+}
+
+const char* ms_last_error(const ms_handle* h) { return h ? h->last_error.c_str() : "null handle"; }
+
+ms_status ms_device_info(char* buf, size_t len) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) {
+        if (buf && len) std::snprintf(buf, len, "no device: %s", cudaGetErrorString(e));
+        return MS_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp p{};
+    cudaGetDeviceProperties(&p, dev);
+    if (buf && len)
+        std::snprintf(buf, len, "%s sm_%d%d, %d SMs, %.1f GB", p.name, p.major, p.minor, p.multiProcessorCount,
+                      p.totalGlobalMem / 1e9);
+    return MS_OK;
+}
+
+ms_status ms_create(const ms_mesh_desc* d, const ms_params* prm, int device, int precision, ms_handle** out) {
+    if (!out) return MS_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (!d || !prm || d->num_nodes <= 0 || d->num_tris <= 0 || !d->patch_ids || !d->deriv_coeffs || !d->ref_area ||
+        !d->ref_thickness || !d->ref_shear_modulus || !d->node_mass || !d->is_constrained)
+        return MS_ERR_INVALID_ARGUMENT;
+    if (precision != MS_PRECISION_FP64 && precision != MS_PRECISION_MIXED) return MS_ERR_INVALID_ARGUMENT;
+    const int N = d->num_nodes, T = d->num_tris;
+    for (long long k = 0; k < 6LL * T; ++k)
+        if (d->patch_ids[k] < 0 || d->patch_ids[k] >= N) return MS_ERR_INVALID_ARGUMENT;
+    if ((long long)6 * T >= (1LL << 31)) return MS_ERR_UNSUPPORTED;
+
+    ms_handle* h = new ms_handle();
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        delete h;
+        return MS_ERR_NO_DEVICE;
+    }
+    if (device >= 0) {
+        if (device >= ndev) {
+            delete h;
+            return MS_ERR_INVALID_ARGUMENT;
+        }
+        cudaSetDevice(device);
+    }
+    cudaGetDevice(&h->device);
+    h->precision = precision;
+    h->params = *prm;
+    h->rho_hh = prm->ref_density * prm->min_ref_thickness * prm->min_ref_thickness;
+    h->force_limit = 50000.0 * prm->char_force_scale;
+    auto bail = [&](ms_status st) {
+        ms_destroy(h);
+        return st;
+    };
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return bail(MS_ERR_CUDA);
+
+    DevMesh& m = h->m;
+    DevState& s = h->s;
+    m.N = N;
+    m.T = T;
+    m.nu = prm->def_poisson_ratio;
+    m.gamma = prm->bend_stiffening_scale_factor;
+    int* patch;
+    double *coef, *area, *thick, *shear, *mass;
+    unsigned char *fixed, *boundary = nullptr;
+    ms_status st;
+    if ((st = dalloc(h, &patch, 6ULL * T)) || (st = dalloc(h, &coef, 24ULL * T)) || (st = dalloc(h, &area, T)) ||
+        (st = dalloc(h, &thick, T)) || (st = dalloc(h, &shear, T)) || (st = dalloc(h, &mass, N)) ||
+        (st = dalloc(h, &fixed, N)))
+        return bail(st);
+    if ((st = upload_transposed<int>(h, patch, d->patch_ids, T, 6)) ||
+        (st = upload_transposed<double>(h, coef, d->deriv_coeffs, T, 24)))
+        return bail(st);
+    if (cudaMemcpy(area, d->ref_area, sizeof(double) * T, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(thick, d->ref_thickness, sizeof(double) * T, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(shear, d->ref_shear_modulus, sizeof(double) * T, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(mass, d->node_mass, sizeof(double) * N, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(fixed, d->is_constrained, N, cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(MS_ERR_CUDA);
+    if (d->is_boundary) {
+        if ((st = dalloc(h, &boundary, N))) return bail(st);
+        if (cudaMemcpy(boundary, d->is_boundary, N, cudaMemcpyHostToDevice) != cudaSuccess) return bail(MS_ERR_CUDA);
+    }
+    m.patch = patch;
+    m.coef = coef;
+    m.area = area;
+    m.thick = thick;
+    m.shear = shear;
+    m.mass = mass;
+    m.fixed = fixed;
+    m.boundary = boundary;
+    bool uniform = true;
+    for (int t = 1; t < T && uniform; ++t)
+        uniform = d->ref_thickness[t] == d->ref_thickness[0] && d->ref_shear_modulus[t] == d->ref_shear_modulus[0];
+    m.uniform_hmu = uniform ? 1 : 0;
+    m.h_uniform = d->ref_thickness[0];
+    m.mu_uniform = d->ref_shear_modulus[0];
+
+    // Incidence lists: node -> (6t + slot), ascending t.
+    {
+        std::vector<int> off(N + 1, 0), ent(6ULL * T);
+        for (long long k = 0; k < 6LL * T; ++k) off[d->patch_ids[k] + 1] += 1;
+        for (int n = 0; n < N; ++n) off[n + 1] += off[n];
+        std::vector<int> fill(off.begin(), off.end() - 1);
+        for (int t = 0; t < T; ++t)
+            for (int k = 0; k < 6; ++k) ent[fill[d->patch_ids[6 * t + k]]++] = 6 * t + k;
+        int *doff, *dent;
+        if ((st = dalloc(h, &doff, N + 1)) || (st = dalloc(h, &dent, 6ULL * T))) return bail(st);
+        if (cudaMemcpy(doff, off.data(), sizeof(int) * (N + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(dent, ent.data(), sizeof(int) * 6 * (size_t)T, cudaMemcpyHostToDevice) != cudaSuccess)
+            return bail(MS_ERR_CUDA);
+        m.inc_off = doff;
+        m.inc_ent = dent;
+    }
+    // Programmed tensors: flat reference state until ms_set_programmed.
+    double *abar, *bbar, *a0, *b0;
+    if ((st = dalloc(h, &abar, 3ULL * T)) || (st = dalloc(h, &bbar, 3ULL * T)) || (st = dalloc(h, &a0, 3ULL * T)) ||
+        (st = dalloc(h, &b0, 3ULL * T)))
+        return bail(st);
+    {
+        std::vector<double> ident(3ULL * T, 0.0);
+        for (int t = 0; t < T; ++t) {
+            ident[t] = 1.0;
+            ident[2ULL * T + t] = 1.0;
+        }
+        cudaMemcpy(abar, ident.data(), sizeof(double) * 3 * T, cudaMemcpyHostToDevice);
+        cudaMemcpy(a0, ident.data(), sizeof(double) * 3 * T, cudaMemcpyHostToDevice);
+        cudaMemset(bbar, 0, sizeof(double) * 3 * T);
+        cudaMemset(b0, 0, sizeof(double) * 3 * T);
+    }
+    m.abar = abar;
+    m.bbar = bbar;
+    m.a0 = a0;
+    m.b0 = b0;
+
+    // State and work buffers.
+    for (int b = 0; b < 2; ++b) {
+        if ((st = dalloc(h, &s.pos[b], 3ULL * N)) || (st = dalloc(h, &s.vel[b], 3ULL * N))) return bail(st);
+        cudaMemset(s.pos[b], 0, sizeof(double) * 3 * N);
+        cudaMemset(s.vel[b], 0, sizeof(double) * 3 * N);
+    }
+    if ((st = dalloc(h, &s.forces, 3ULL * N)) || (st = dalloc(h, &s.cq, 15ULL * T)) ||
+        (st = dalloc(h, &s.dEdcq, 15ULL * T)) || (st = dalloc(h, &s.contrib, 18ULL * T)) ||
+        (st = dalloc(h, &s.err, 1)) || (st = dalloc(h, &s.equil, 1)))
+        return bail(st);
+    cudaMemset(s.forces, 0, sizeof(double) * 3 * N);
+    s.eq_blocks = (N + 255) / 256;
+    if ((st = dalloc(h, &s.eq_part, s.eq_blocks)) || (st = dalloc(h, &s.eq_counter, 1))) return bail(st);
+    cudaMemset(s.eq_counter, 0, sizeof(unsigned int));
+    if ((st = dalloc(h, &h->d_scratch_tri, 2ULL * T)) || (st = dalloc(h, &h->d_scratch_node, N)) ||
+        (st = dalloc(h, &h->d_sum_partial, 1024)) || (st = dalloc(h, &h->d_sums, 4)))
+        return bail(st);
+    if (precision == MS_PRECISION_MIXED) {
+        float *coef_f, *area_f, *contrib_f;
+        if ((st = dalloc(h, &coef_f, 24ULL * T)) || (st = dalloc(h, &area_f, T)) ||
+            (st = dalloc(h, &contrib_f, 18ULL * T)))
+            return bail(st);
+        std::vector<float> cf(24ULL * T), af(T);
+        for (int t = 0; t < T; ++t) {
+            af[t] = (float)d->ref_area[t];
+            for (int k = 0; k < 24; ++k) cf[(size_t)k * T + t] = (float)d->deriv_coeffs[24ULL * t + k];
+        }
+        cudaMemcpy(coef_f, cf.data(), sizeof(float) * cf.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(area_f, af.data(), sizeof(float) * T, cudaMemcpyHostToDevice);
+        m.coef_f = coef_f;
+        m.area_f = area_f;
+        m.contrib_f = contrib_f;
+    }
+    if (cudaMallocHost(&h->h_err, sizeof(DevError)) != cudaSuccess ||
+        cudaMallocHost(&h->h_equil, sizeof(DevEquil)) != cudaSuccess)
+        return bail(MS_ERR_CUDA);
+    if (reset_error(h) != MS_OK) return bail(MS_ERR_CUDA);
+    cudaError_t le = cudaStreamSynchronize(h->stream);
+    if (le != cudaSuccess) {
+        cuda_fail(h, le, "ms_create");
+        return bail(MS_ERR_CUDA);
+    }
+    *out = h;
+    return MS_OK;
+}
+
+ms_status ms_destroy(ms_handle* h) {
+    if (!h) return MS_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    clear_graphs(h);
+    for (void* p : h->allocs) cudaFree(p);
+    if (h->h_dials) cudaFreeHost(h->h_dials);
+    if (h->h_err) cudaFreeHost(h->h_err);
+    if (h->h_equil) cudaFreeHost(h->h_equil);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return MS_OK;
+}
+
+ms_status ms_upload_dofs(ms_handle* h, const double* dofs, const double* vel) {
+    if (!h || !dofs) return MS_ERR_INVALID_ARGUMENT;
+    const size_t n3 = 3ULL * h->m.N;
+    MS_CUDA(h, cudaMemcpyAsync(h->s.pos[h->cur], dofs, n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (vel) MS_CUDA(h, cudaMemcpyAsync(h->s.vel[h->cur], vel, n3 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    else MS_CUDA(h, cudaMemsetAsync(h->s.vel[h->cur], 0, n3 * sizeof(double), h->stream));
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MS_OK;
+}
+
+ms_status ms_download_dofs(ms_handle* h, double* dofs, double* vel) {
+    if (!h) return MS_ERR_INVALID_ARGUMENT;
+    const size_t n3 = 3ULL * h->m.N;
+    if (dofs) MS_CUDA(h, cudaMemcpyAsync(dofs, h->s.pos[h->cur], n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (vel) MS_CUDA(h, cudaMemcpyAsync(vel, h->s.vel[h->cur], n3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MS_OK;
+}
+
+ms_status ms_download_forces(ms_handle* h, double* forces) {
+    if (!h || !forces) return MS_ERR_INVALID_ARGUMENT;
+    MS_CUDA(h, cudaMemcpyAsync(forces, h->s.forces, 3ULL * h->m.N * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MS_OK;
+}
+
+ms_status ms_set_programmed(ms_handle* h, int protocol, const double* abar_info, int ka, const double* bbar_info,
+                            int kb, double spacing, int from_ansatz) {
+    if (!h || !abar_info || !bbar_info || ka <= 0 || kb <= 0) return MS_ERR_INVALID_ARGUMENT;
+    const int need_a[6] = {0, 3, 3, 3, 13, 1};
+    const int need_b[6] = {0, 3, 3, 1, 1, 1};
+    if (protocol < 1 || protocol > 5) return fail(h, MS_ERR_INVALID_ARGUMENT, "protocol must be 1..5");
+    if (ka < need_a[protocol] || kb < need_b[protocol])
+        return fail(h, MS_ERR_INVALID_ARGUMENT, "abar_info/bbar_info have too few columns for this protocol");
+    if (protocol == 4 && !(spacing > 0)) return fail(h, MS_ERR_INVALID_ARGUMENT, "protocol 4 needs spacing > 0");
+    const size_t T = h->m.T;
+    if (h->m.info_a) {
+        cudaFree((void*)h->m.info_a);
+        h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->m.info_a), h->allocs.end());
+    }
+    if (h->m.info_b) {
+        cudaFree((void*)h->m.info_b);
+        h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->m.info_b), h->allocs.end());
+    }
+    double *ia, *ib;
+    MS_TRY(dalloc(h, &ia, T * ka));
+    MS_TRY(dalloc(h, &ib, T * kb));
+    MS_TRY(upload_transposed<double>(h, ia, abar_info, T, ka));
+    MS_TRY(upload_transposed<double>(h, ib, bbar_info, T, kb));
+    h->m.info_a = ia;
+    h->m.info_b = ib;
+    h->m.ka = ka;
+    h->m.kb = kb;
+    h->protocol = protocol;
+    h->spacing = spacing;
+    h->from_ansatz = from_ansatz ? 1 : 0;
+    h->programmed = true;
+    clear_graphs(h);  // graphs bake the mesh struct
+    return MS_OK;
+}
+
+ms_status ms_set_zero_dial_state(ms_handle* h, const double* a0, const double* b0) {
+    if (!h) return MS_ERR_INVALID_ARGUMENT;
+    const size_t T = h->m.T;
+    std::vector<double> ident(3 * T, 0.0);
+    for (size_t t = 0; t < T; ++t) {
+        ident[t] = 1.0;
+        ident[2 * T + t] = 1.0;
+    }
+    if (a0) MS_TRY(upload_transposed<double>(h, (double*)h->m.a0, a0, T, 3));
+    else MS_CUDA(h, cudaMemcpy((void*)h->m.a0, ident.data(), 3 * T * sizeof(double), cudaMemcpyHostToDevice));
+    if (b0) MS_TRY(upload_transposed<double>(h, (double*)h->m.b0, b0, T, 3));
+    else MS_CUDA(h, cudaMemset((void*)h->m.b0, 0, 3 * T * sizeof(double)));
+    return MS_OK;
+}
+
+ms_status ms_do_dialling(ms_handle* h, double dial) {
+    if (!h) return MS_ERR_INVALID_ARGUMENT;
+    if (!h->programmed) return fail(h, MS_ERR_INVALID_ARGUMENT, "ms_set_programmed has not been called");
+    MS_CUDA(h, launch_dialling(h->m, h->protocol, dial, h->spacing, h->from_ansatz, h->stream));
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MS_OK;
+}
+
+ms_status ms_download_programmed(ms_handle* h, double* abar, double* bbar) {
+    if (!h) return MS_ERR_INVALID_ARGUMENT;
+    if (abar) MS_TRY(download_transposed<double>(h, abar, h->m.abar, h->m.T, 3));
+    if (bbar) MS_TRY(download_transposed<double>(h, bbar, h->m.bbar, h->m.T, 3));
+    return MS_OK;
+}
+
+ms_status ms_surface_derivs(ms_handle* h, double* cq) {
+    if (!h) return MS_ERR_INVALID_ARGUMENT;
+    MS_CUDA(h, launch_surface_derivs(h->m, h->s, h->cur, h->stream));
+    if (cq)
+        MS_CUDA(h, cudaMemcpyAsync(cq, h->s.cq, 15ULL * h->m.T * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MS_OK;
+}
+
+ms_status ms_a_b_normals(ms_handle* h, double* a, double* b, double* n) {
+    if (!h || !a || !b || !n) return MS_ERR_INVALID_ARGUMENT;
+    const size_t T = h->m.T;
+    MS_TRY(ensure_out(h, 9 * T * sizeof(double)));
+    double* da = h->d_out;
+    MS_CUDA(h, launch_a_b_normals(h->m, h->s, da, da + 3 * T, da + 6 * T, h->stream));
+    MS_CUDA(h, cudaMemcpyAsync(a, da, 3 * T * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MS_CUDA(h, cudaMemcpyAsync(b, da + 3 * T, 3 * T * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MS_CUDA(h, cudaMemcpyAsync(n, da + 6 * T, 3 * T * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MS_OK;
+}
+
+ms_status ms_deformation_forces(ms_handle* h, double* forces, double* dE) {
+    if (!h) return MS_ERR_INVALID_ARGUMENT;
+    MS_CUDA(h, launch_forces_from_cq(h->m, h->s, dE ? 1 : 0, h->stream));
+    MS_CUDA(h, launch_gather_forces(h->m, h->s, h->stream));
+    if (forces)
+        MS_CUDA(h, cudaMemcpyAsync(forces, h->s.forces, 3ULL * h->m.N * sizeof(double), cudaMemcpyDeviceToHost,
+                                   h->stream));
+    if (dE)
+        MS_CUDA(h, cudaMemcpyAsync(dE, h->s.dEdcq, 15ULL * h->m.T * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MS_OK;
+}
+
+ms_status ms_non_deformation_forces(ms_handle* h, double damping, int gd) {
+    if (!h) return MS_ERR_INVALID_ARGUMENT;
+    if (!gd) MS_CUDA(h, launch_damping(h->m, h->s, h->cur, damping, h->rho_hh, h->stream));
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MS_OK;
+}
+
+ms_status ms_impose_constraints(ms_handle* h) {
+    if (!h) return MS_ERR_INVALID_ARGUMENT;
+    MS_CUDA(h, launch_constraints(h->m, h->s, h->stream));
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MS_OK;
+}
+
+static void fill_equil(const ms_handle* h, const DevEquil& e, ms_equil_result* out) {
+    out->max_force = e.max_force;
+    out->max_speed = e.max_speed;
+    out->max_force_node = e.max_force_node;
+    out->max_speed_node = e.max_speed_node;
+    out->at_equilibrium = (e.max_force / h->params.char_force_scale) < h->params.force_to_char_force_ratio_equil_threshold &&
+                          (e.max_speed / h->params.char_speed_scale) < h->params.speed_to_char_speed_ratio_equil_threshold;
+}
+
+ms_status ms_is_at_equilibrium(ms_handle* h, ms_equil_result* out) {
+    if (!h || !out) return MS_ERR_INVALID_ARGUMENT;
+    MS_CUDA(h, launch_equilibrium(h->m, h->s, h->cur, h->stream));
+    MS_CUDA(h, cudaMemcpyAsync(h->h_equil, h->s.equil, sizeof(DevEquil), cudaMemcpyDeviceToHost, h->stream));
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    fill_equil(h, *h->h_equil, out);
+    return MS_OK;
+}
+
+ms_status ms_advance_dynamics(ms_handle* h, double dt, double damping, int gd, int64_t* bad_dof, double* bad_force) {
+    if (!h) return MS_ERR_INVALID_ARGUMENT;
+    if (bad_dof) *bad_dof = -1;
+    MS_TRY(reset_error(h));
+    MS_CUDA(h, launch_guard(h->m, h->s, h->force_limit, h->stream));
+    MS_CUDA(h, cudaMemcpyAsync(h->h_err, h->s.err, sizeof(DevError), cudaMemcpyDeviceToHost, h->stream));
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (h->h_err->flag) {
+        const long long d = (long long)(h->h_err->guard_key & 0xffffffffULL);
+        double f = 0;
+        cudaMemcpy(&f, h->s.forces + d, sizeof(double), cudaMemcpyDeviceToHost);
+        if (bad_dof) *bad_dof = d;
+        if (bad_force) *bad_force = f;
+        return fail(h, MS_ERR_IMPLAUSIBLE_FORCE, "implausibly_high_force");
+    }
+    MS_CUDA(h, launch_advance(h->m, h->s, h->cur, dt, damping, h->rho_hh, gd, h->stream));
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MS_OK;
+}
+
+ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, double dt, double damping, int gd,
+                    int check_last, ms_step_report* rep) {
+    if (!h || n < 0) return MS_ERR_INVALID_ARGUMENT;
+    if (rep) {
+        std::memset(rep, 0, sizeof(*rep));
+        rep->error_step = -1;
+        rep->offending_dof = -1;
+    }
+    if (n == 0) return MS_OK;
+    if (dialling && (!dials || !h->programmed))
+        return fail(h, MS_ERR_INVALID_ARGUMENT, "dialling steps need dial factors and ms_set_programmed");
+    const bool fuse_lce = dialling && lce_fusable(h);
+    const int dial_mode = fuse_lce ? DIAL_LCE : DIAL_ARRAYS;
+    cudaStream_t st = h->stream;
+
+    if (dialling) {
+        if (h->dials_cap < n) {
+            if (h->d_dials) {
+                cudaFree(h->d_dials);
+                h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->d_dials), h->allocs.end());
+            }
+            int cap = std::max(n, 1024);
+            MS_TRY(dalloc(h, &h->d_dials, cap));
+            h->dials_cap = cap;
+            h->s.dials = h->d_dials;
+            clear_graphs(h);
+        }
+        if (h->h_dials_cap < n) {
+            if (h->h_dials) cudaFreeHost(h->h_dials);
+            int cap = std::max(n, 1024);
+            MS_CUDA(h, cudaMallocHost(&h->h_dials, cap * sizeof(double)));
+            h->h_dials_cap = cap;
+        }
+        MS_CUDA(h, cudaStreamSynchronize(st));
+        std::memcpy(h->h_dials, dials, n * sizeof(double));
+        MS_CUDA(h, cudaMemcpyAsync(h->d_dials, h->h_dials, n * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+    MS_TRY(reset_error(h));
+    const int p0 = h->cur;
+    int done = 0;
+    while (done < n) {
+        const int len = std::min(kChunk, n - done);
+        const bool last_chunk = done + len == n;
+        GraphKey key{len, p0 ^ (done & 1), dial_mode, gd, (check_last && last_chunk) ? 1 : 0, dt, damping};
+        cudaGraphExec_t exec = nullptr;
+        if (!(dialling && !fuse_lce))
+            for (auto& g : h->graphs)
+                if (g.key == key) {
+                    exec = g.exec;
+                    g.last_use = ++h->use_clock;
+                }
+        if (!exec) {
+            // Non-LCE dialling materialises abar/bbar with the dialling kernel
+            // each step; that kernel takes the dial factor by value, so those
+            // segments are launched directly instead of through a graph.
+            if (dialling && !fuse_lce) {
+                for (int i = 0; i < len; ++i) {
+                    MS_CUDA(h, launch_dialling(h->m, h->protocol, dials[done + i], h->spacing, h->from_ansatz, st));
+                    StepScalars sc{i, key.parity ^ (i & 1), dt, damping, h->rho_hh, h->force_limit, gd,
+                                   (key.check_last && i == len - 1) ? 1 : 0};
+                    MS_CUDA(h, launch_tri_fused(h->m, h->s, sc, DIAL_ARRAYS, h->precision, st));
+                    MS_CUDA(h, launch_node_update(h->m, h->s, sc, h->precision, st));
+                }
+                MS_CUDA(h, launch_chunk_end(h->s, len, st));
+                done += len;
+                continue;
+            }
+            cudaGraph_t graph;
+            MS_CUDA(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            cudaError_t ce = cudaSuccess;
+            for (int i = 0; i < len && ce == cudaSuccess; ++i) {
+                StepScalars sc{i, key.parity ^ (i & 1), dt, damping, h->rho_hh, h->force_limit, gd,
+                               (key.check_last && i == len - 1) ? 1 : 0};
+                ce = launch_tri_fused(h->m, h->s, sc, dial_mode, h->precision, st);
+                if (ce == cudaSuccess) ce = launch_node_update(h->m, h->s, sc, h->precision, st);
+            }
+            if (ce == cudaSuccess) ce = launch_chunk_end(h->s, len, st);
+            cudaError_t ee = cudaStreamEndCapture(st, &graph);
+            if (ce != cudaSuccess) return cuda_fail(h, ce, "capture");
+            if (ee != cudaSuccess) return cuda_fail(h, ee, "cudaStreamEndCapture");
+            ee = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ee != cudaSuccess) return cuda_fail(h, ee, "cudaGraphInstantiate");
+            if (h->graphs.size() >= 8) {
+                auto it = std::min_element(h->graphs.begin(), h->graphs.end(),
+                                           [](const GraphEntry& a, const GraphEntry& b) { return a.last_use < b.last_use; });
+                cudaGraphExecDestroy(it->exec);
+                h->graphs.erase(it);
+            }
+            h->graphs.push_back({key, exec, ++h->use_clock});
+        }
+        MS_CUDA(h, cudaGraphLaunch(exec, st));
+        done += len;
+    }
+    MS_CUDA(h, cudaMemcpyAsync(h->h_err, h->s.err, sizeof(DevError), cudaMemcpyDeviceToHost, st));
+    if (check_last) MS_CUDA(h, cudaMemcpyAsync(h->h_equil, h->s.equil, sizeof(DevEquil), cudaMemcpyDeviceToHost, st));
+    MS_CUDA(h, cudaStreamSynchronize(st));
+    if (h->h_err->flag) {
+        const unsigned long long key = h->h_err->guard_key;
+        const int step = (int)(key >> 32);
+        const long long dof = (long long)(key & 0xffffffffULL);
+        h->cur = p0 ^ (step & 1);
+        // Recompute the failing step's forces from its saved input state, as
+        // the reference holds them when it throws (main.cpp:448-474).
+        if (dialling) MS_CUDA(h, launch_dialling(h->m, h->protocol, dials[step], h->spacing, h->from_ansatz, st));
+        MS_CUDA(h, launch_surface_derivs(h->m, h->s, h->cur, st));
+        MS_CUDA(h, launch_forces_from_cq(h->m, h->s, 0, st));
+        MS_CUDA(h, launch_gather_forces(h->m, h->s, st));
+        if (!gd) MS_CUDA(h, launch_damping(h->m, h->s, h->cur, damping, h->rho_hh, st));
+        MS_CUDA(h, launch_constraints(h->m, h->s, st));
+        double f = 0.0;
+        MS_CUDA(h, cudaMemcpyAsync(&f, h->s.forces + dof, sizeof(double), cudaMemcpyDeviceToHost, st));
+        MS_CUDA(h, cudaStreamSynchronize(st));
+        if (rep) {
+            rep->steps_done = step;
+            rep->error_step = step;
+            rep->offending_dof = dof;
+            rep->offending_force = f;
+        }
+        return fail(h, MS_ERR_IMPLAUSIBLE_FORCE, "implausibly_high_force");
+    }
+    // The fused LCE path never wrote abar/bbar; leave the tensors of the last
+    // dialled step in force, as do_dialling would have.
+    if (fuse_lce) {
+        MS_CUDA(h, launch_dialling(h->m, h->protocol, dials[n - 1], h->spacing, h->from_ansatz, st));
+        MS_CUDA(h, cudaStreamSynchronize(st));
+    }
+    h->cur = p0 ^ (n & 1);
+    if (rep) {
+        rep->steps_done = n;
+        if (check_last) fill_equil(h, *h->h_equil, &rep->equil);
+    }
+    return MS_OK;
+}
+
+ms_status ms_output_quantities(ms_handle* h, double* curv, double* edens, double* strains, double* stresses,
+                               double* deficits, double* energies) {
+    if (!h) return MS_ERR_INVALID_ARGUMENT;
+    const size_t T = h->m.T, N = h->m.N;
+    cudaStream_t st = h->stream;
+    MS_CUDA(h, launch_surface_derivs(h->m, h->s, h->cur, st));
+    MS_TRY(ensure_out(h, (2 * T + 2 * T + T + 8 * T + N) * sizeof(double)));
+    double* dcurv = h->d_out;
+    double* dedens = dcurv + 2 * T;
+    double* dstrain = dedens + 2 * T;
+    double* dstress = dstrain + T;
+    double* ddef = dstress + 8 * T;
+    MS_CUDA(h, launch_output_tri(h->m, h->s, dcurv, dedens, dstrain, dstress, h->d_scratch_tri, st));
+    if (deficits) MS_CUDA(h, launch_angle_deficits(h->m, h->s, h->cur, ddef, st));
+    if (energies) {
+        MS_CUDA(h, launch_kinetic(h->m, h->s, h->cur, h->d_scratch_node, st));
+        MS_CUDA(h, launch_comp_sum(h->d_scratch_tri, (int)T, h->d_sum_partial, h->d_sums + 0, st));
+        MS_CUDA(h, launch_comp_sum(h->d_scratch_tri + T, (int)T, h->d_sum_partial, h->d_sums + 1, st));
+        MS_CUDA(h, launch_comp_sum(h->d_scratch_node, (int)N, h->d_sum_partial, h->d_sums + 2, st));
+        MS_CUDA(h, cudaMemcpyAsync(energies, h->d_sums, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+    if (curv) MS_CUDA(h, cudaMemcpyAsync(curv, dcurv, 2 * T * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (edens) MS_CUDA(h, cudaMemcpyAsync(edens, dedens, 2 * T * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (strains) MS_CUDA(h, cudaMemcpyAsync(strains, dstrain, T * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (stresses) MS_CUDA(h, cudaMemcpyAsync(stresses, dstress, 8 * T * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (deficits) MS_CUDA(h, cudaMemcpyAsync(deficits, ddef, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+    MS_CUDA(h, cudaStreamSynchronize(st));
+    return MS_OK;
+}
+
+}  // extern "C"

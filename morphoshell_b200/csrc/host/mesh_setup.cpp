@@ -1,0 +1,446 @@
+// One-off mesh set-up: topology, patch fitting, derivative coefficients,
+// lumped masses and the characteristic scales that fix dt, damping and the
+// dialling schedule.  Each function follows the reference file named above
+// it; the formulas are kept term for term so that the scalars (and hence dt
+// and the step counts) come out the same.
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <iterator>
+#include <random>
+
+#include "host.hpp"
+#include "small_linalg.hpp"
+
+namespace msb {
+
+namespace {
+
+inline double norm3(double x, double y, double z) { return std::sqrt(x * x + y * y + z * z); }
+
+double vmin(const std::vector<double>& v, size_t* arg = nullptr) {
+    auto it = std::min_element(v.begin(), v.end());
+    if (arg) *arg = static_cast<size_t>(std::distance(v.begin(), it));
+    return *it;
+}
+double vmax(const std::vector<double>& v, size_t* arg = nullptr) {
+    auto it = std::max_element(v.begin(), v.end());
+    if (arg) *arg = static_cast<size_t>(std::distance(v.begin(), it));
+    return *it;
+}
+
+}  // namespace
+
+// source_files/kahan_sum.cpp:32-49
+double kahan_sum(const std::vector<double>& vec) {
+    double sum = 0.0, comp = 0.0;
+    for (double x : vec) {
+        volatile double y = x - comp;
+        volatile double t = sum + y;
+        comp = (t - sum) - y;
+        sum = t;
+    }
+    return sum;
+}
+
+// calc_triangles_incident_on_nodes.cpp:47-53, calc_node_neighbours.cpp,
+// calc_triangle_adjacencies.cpp, calc_edges.cpp and calc_mesh_info.cpp:50-185.
+void calc_mesh_info(std::vector<Node>& nodes, const DMat& P, std::vector<Tri>& triangles, std::vector<Edge>& edges,
+                    Stuff& stuff, Log& log) {
+    // Incident triangles, in triangle order.
+    for (auto& node : nodes) node.incident_tri_ids.clear();
+    for (const auto& tri : triangles)
+        for (int v : tri.vertex_ids) nodes.at(v).incident_tri_ids.push_back(tri.id);
+    // 1-rings, sorted and unique.
+    for (auto& node : nodes) {
+        node.neighbour_node_ids.clear();
+        for (int t : node.incident_tri_ids)
+            for (int v : triangles[t].vertex_ids)
+                if (v != node.id) node.neighbour_node_ids.push_back(v);
+        std::sort(node.neighbour_node_ids.begin(), node.neighbour_node_ids.end());
+        node.neighbour_node_ids.erase(std::unique(node.neighbour_node_ids.begin(), node.neighbour_node_ids.end()),
+                                      node.neighbour_node_ids.end());
+    }
+    // Edge-sharing triangles.
+    for (auto& tri : triangles) {
+        std::vector<int> cand;
+        for (int v : tri.vertex_ids)
+            for (int t : nodes[v].incident_tri_ids)
+                if (t != tri.id) cand.push_back(t);
+        std::sort(cand.begin(), cand.end());
+        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+        tri.edge_sharing_tri_ids.clear();
+        for (int t : cand) {
+            int common = 0;
+            for (int a : tri.vertex_ids)
+                for (int b : triangles[t].vertex_ids) common += (a == b);
+            if (common == 2) tri.edge_sharing_tri_ids.push_back(t);
+        }
+    }
+    for (const auto& tri : triangles)
+        if (tri.edge_sharing_tri_ids.size() < 1 || tri.edge_sharing_tri_ids.size() > 3)
+            throw std::runtime_error(
+                "Error: Problem with triangle (edge-sharing) adjacencies or edges setup. "
+                "Either there is a bug, or some mesh pathology; investigate further!");
+    // Edges (i, j), i < j, in lexicographic order.
+    edges.clear();
+    edges.reserve(3 * static_cast<size_t>(stuff.num_tris));
+    for (const auto& node : nodes)
+        for (int nb : node.neighbour_node_ids)
+            if (nb > node.id) {
+                Edge e;
+                e.node_ids = {node.id, nb};
+                if (edges.size() >= static_cast<size_t>(INT_MAX))
+                    throw std::overflow_error("edge count overflowed int");
+                e.id = static_cast<int>(edges.size());
+                edges.push_back(e);
+            }
+    stuff.num_edges = static_cast<int>(edges.size());
+    for (auto& e : edges) {
+        std::vector<int> a = nodes[e.node_ids[0]].incident_tri_ids, b = nodes[e.node_ids[1]].incident_tri_ids;
+        std::sort(a.begin(), a.end());
+        std::sort(b.begin(), b.end());
+        std::vector<int> common;
+        std::set_intersection(a.begin(), a.end(), b.begin(), b.end(), std::back_inserter(common));
+        if (common.size() == 1) {
+            e.is_boundary = true;
+            e.adjacent_tri_ids = common;
+        } else if (common.size() == 2) {
+            e.is_boundary = false;
+            e.adjacent_tri_ids = common;
+        } else {
+            throw std::runtime_error(
+                "Something has gone very wrong in calc_edges, because the nodes at each end of an edge "
+                "should have either one or two incident triangles in common, but the code thinks it's "
+                "found an exception. Investigate!");
+        }
+    }
+    std::vector<int> cursor(stuff.num_tris, 0);
+    for (const auto& e : edges)
+        for (int t : e.adjacent_tri_ids) {
+            if (cursor[t] < 3) triangles[t].edge_ids[cursor[t]] = e.id;
+            cursor[t] += 1;
+        }
+
+    stuff.num_dofs = 3 * stuff.num_nodes;
+    stuff.num_continuum_quantities = 15 * stuff.num_tris;
+    stuff.num_boundary_edges = 0;
+    std::vector<double> bedge_len;
+    for (const auto& e : edges)
+        if (e.is_boundary) {
+            stuff.num_boundary_edges += 1;
+            nodes[e.node_ids[0]].is_boundary = true;
+            nodes[e.node_ids[1]].is_boundary = true;
+            int i = e.node_ids[0], j = e.node_ids[1];
+            bedge_len.push_back(norm3(P(i, 0) - P(j, 0), P(i, 1) - P(j, 1), P(i, 2) - P(j, 2)));
+        }
+    stuff.num_boundary_nodes = 0;
+    for (const auto& node : nodes) stuff.num_boundary_nodes += node.is_boundary ? 1 : 0;
+    for (auto& tri : triangles) {
+        tri.is_boundary = false;
+        for (int v : tri.vertex_ids) tri.is_boundary = tri.is_boundary || nodes[v].is_boundary;
+    }
+    double perimeter = kahan_sum(bedge_len);
+    stuff.sample_char_length = perimeter;
+    log << "Reference perimeter = " << perimeter << std::endl;
+    log << "Number of edges = " << stuff.num_edges << std::endl;
+    log << "Number of boundary edges = " << stuff.num_boundary_edges << std::endl;
+    log << "Number of non-boundary edges = " << stuff.num_edges - stuff.num_boundary_edges << std::endl;
+    log << "Number of holes in mesh = " << 1 + stuff.num_edges - stuff.num_nodes - stuff.num_tris << std::endl;
+    log << "Number of boundary nodes = " << stuff.num_boundary_nodes << std::endl;
+    if (3 * stuff.num_tris != 2 * stuff.num_edges - stuff.num_boundary_edges)
+        throw std::runtime_error(
+            "Something has gone wrong in calculating triangle adjacencies and/or "
+            "edges: the current edge and triangle counts violate a topological identity.");
+    if (1 + stuff.num_edges - stuff.num_nodes - stuff.num_tris < 0)
+        throw std::runtime_error(
+            "Something is very wrong with the mesh, because the code thinks it has a "
+            "negative number of holes! A first thing to check is that all nodes touch at least one tri.");
+
+    // Areas (Tri_Class.cpp:31-36), smallest altitudes, centroids.
+    std::vector<double> areas;
+    for (auto& tri : triangles) {
+        int a = tri.vertex_ids[0], b = tri.vertex_ids[1], c = tri.vertex_ids[2];
+        double s1[3] = {P(b, 0) - P(a, 0), P(b, 1) - P(a, 1), P(b, 2) - P(a, 2)};
+        double s2[3] = {P(c, 0) - P(a, 0), P(c, 1) - P(a, 1), P(c, 2) - P(a, 2)};
+        double cx = 0.5 * (s1[1] * s2[2] - s1[2] * s2[1]);
+        double cy = 0.5 * (s1[2] * s2[0] - s1[0] * s2[2]);
+        double cz = 0.5 * (s1[0] * s2[1] - s1[1] * s2[0]);
+        tri.ref_area = norm3(cx, cy, cz);
+        areas.push_back(tri.ref_area);
+    }
+    stuff.total_ref_area = kahan_sum(areas);
+    std::vector<double> smallest_alt, aspect;
+    for (const auto& tri : triangles) {
+        int a = tri.vertex_ids[0], b = tri.vertex_ids[1], c = tri.vertex_ids[2];
+        double l1 = norm3(P(b, 0) - P(a, 0), P(b, 1) - P(a, 1), P(b, 2) - P(a, 2));
+        double l2 = norm3(P(c, 0) - P(a, 0), P(c, 1) - P(a, 1), P(c, 2) - P(a, 2));
+        double l3 = norm3(P(c, 0) - P(b, 0), P(c, 1) - P(b, 1), P(c, 2) - P(b, 2));
+        std::vector<double> alt{2.0 * tri.ref_area / l1, 2.0 * tri.ref_area / l2, 2.0 * tri.ref_area / l3};
+        double lo = vmin(alt), hi = vmax(alt);
+        smallest_alt.push_back(lo);
+        aspect.push_back(lo / hi);
+    }
+    size_t smallest_tri = 0, worst_tri = 0;
+    stuff.approx_min_tri_size = vmin(smallest_alt, &smallest_tri);
+    double worst = vmin(aspect, &worst_tri);
+    log << "Approx smallest tri linear size = " << stuff.approx_min_tri_size << " (tri " << smallest_tri << ")"
+        << std::endl;
+    log << "Worst tri aspect ratio = " << worst << " (tri " << worst_tri
+        << "). Around 0 is bad, 1 would be perfection." << std::endl;
+    for (auto& tri : triangles)
+        for (int k = 0; k < 3; ++k)
+            tri.ref_centroid[k] = (P(tri.vertex_ids[0], k) + P(tri.vertex_ids[1], k) + P(tri.vertex_ids[2], k)) / 3.0;
+}
+
+// source_files/set_up_patch_fitting.cpp:48-305.  For each triangle, the
+// three extra patch nodes are the nearest candidates (vertices of triangles
+// incident on its vertices, nearest first) whose 6x6 quadratic-fit matrix is
+// invertible and well conditioned; the kept 6x3 block maps the six patch
+// nodes' values to the second derivatives (xx, xy, yy) at the centroid.
+void set_up_patch_fitting(const std::vector<Node>& nodes, const DMat& P, std::vector<Tri>& triangles,
+                          const Stuff& stuff, Log& log) {
+    int num_interior_retries = 0;
+    for (auto& tri : triangles) {
+        std::vector<double> dists;
+        std::vector<int> cands;
+        for (int v = 0; v < 3; ++v)
+            for (int it : nodes[tri.vertex_ids[v]].incident_tri_ids)
+                for (int w = 0; w < 3; ++w) {
+                    int id = triangles[it].vertex_ids[w];
+                    bool seen = (id == tri.vertex_ids[0] || id == tri.vertex_ids[1] || id == tri.vertex_ids[2]);
+                    for (int c : cands) seen = seen || (c == id);
+                    if (!seen) {
+                        dists.push_back(norm3(P(id, 0) - tri.ref_centroid[0], P(id, 1) - tri.ref_centroid[1],
+                                              P(id, 2) - tri.ref_centroid[2]));
+                        cands.push_back(id);
+                    }
+                }
+        if (cands.size() < 3)
+            throw std::runtime_error("At least one search for patch nodes was exhausted without success (triangle " +
+                                     std::to_string(tri.id) + "): fewer than 3 candidate patch nodes.");
+        std::vector<size_t> order(dists.size());
+        for (size_t q = 0; q < order.size(); ++q) order[q] = q;
+        std::sort(order.begin(), order.end(), [&dists](const size_t& a, const size_t& b) { return dists[a] < dists[b]; });
+        tri.non_vertex_patch_nodes_ids[0] = cands[order[0]];
+        bool success = false;
+        for (size_t p = 1; p < std::min<size_t>(4, order.size()) && !success; ++p) {
+            tri.non_vertex_patch_nodes_ids[1] = cands[order[p]];
+            for (size_t q = 2; q < cands.size(); ++q) {
+                tri.non_vertex_patch_nodes_ids[2] = cands[order[q]];
+                int ids[6] = {tri.vertex_ids[0], tri.vertex_ids[1], tri.vertex_ids[2],
+                              tri.non_vertex_patch_nodes_ids[0], tri.non_vertex_patch_nodes_ids[1],
+                              tri.non_vertex_patch_nodes_ids[2]};
+                double sq = 0.0;
+                for (int n = 0; n < 6; ++n) {
+                    double dx = P(ids[n], 0) - tri.ref_centroid[0], dy = P(ids[n], 1) - tri.ref_centroid[1],
+                           dz = P(ids[n], 2) - tri.ref_centroid[2];
+                    sq += dx * dx + dy * dy + dz * dz;
+                }
+                double patch_size = std::sqrt(sq / 6.0);
+                double m[6][6];
+                for (int n = 0; n < 6; ++n) {
+                    double dx = P(ids[n], 0) - tri.ref_centroid[0];
+                    double dy = P(ids[n], 1) - tri.ref_centroid[1];
+                    m[0][n] = 1.0;
+                    m[1][n] = dx;
+                    m[2][n] = dy;
+                    m[3][n] = 0.5 * dx * dx;
+                    m[4][n] = dx * dy;
+                    m[5][n] = 0.5 * dy * dy;
+                }
+                bool accepted = false;
+                double block[6][3];
+                if (la::full_piv_rank<6>(m) == 6) {
+                    double inv[6][6];
+                    if (la::inverse_partial_piv<6>(m, inv)) {
+                        for (int r = 0; r < 6; ++r)
+                            for (int c = 0; c < 3; ++c) block[r][c] = inv[r][3 + c];
+                        double sigma = la::max_singular_value_6x3(block);
+                        double ratio = sigma * patch_size * patch_size / stuff.patch_mat_dimless_conditioning_thresh;
+                        accepted = ratio < 1.0;
+                    }
+                }
+                if (!accepted) {
+                    if (q == 2 && !tri.is_boundary) num_interior_retries += 1;
+                    continue;
+                }
+                for (int r = 0; r < 6; ++r)
+                    for (int c = 0; c < 3; ++c) tri.mat_for_patch_2nd_derivs[r][c] = block[r][c];
+                success = true;
+                break;
+            }
+        }
+        if (!success)
+            throw std::runtime_error(
+                "At least one search for patch nodes was exhausted without success (triangle " +
+                std::to_string(tri.id) +
+                "); all possible patch matrices in the search had a  condition number above the acceptance "
+                "threshold. Try increasing this threshold. If that does not solve the issue, or causes other "
+                "issues, either the patch node search will need to be extended, or you will need to use a nicer "
+                "mesh. Aborting.");
+    }
+    log << "\nNumber of non-boundary triangles that had to search through \n"
+        << "multiple possible patch options to find one \nsatisfying the condition number "
+        << "criterion was " << num_interior_retries << ", \nwhich should not be a large proportion of the mesh's "
+        << "triangles." << std::endl;
+}
+
+// source_files/calc_deriv_mats.cpp:46-136, kept as a dense per-triangle table
+// instead of the sparse num_cq x num_dofs matrix: first-derivative weights
+// from the inverse of the linear-interpolation matrix, second-derivative
+// weights from the patch fit.
+void calc_deriv_coeffs(std::vector<double>& coeffs, const DMat& P, const std::vector<Tri>& triangles,
+                       const Stuff& stuff) {
+    coeffs.assign(static_cast<size_t>(stuff.num_tris) * 24, 0.0);
+    for (const auto& tri : triangles) {
+        double a[3][3], inv[3][3];
+        for (int v = 0; v < 3; ++v) {
+            a[v][0] = 1.0;
+            a[v][1] = P(tri.vertex_ids[v], 0) - tri.ref_centroid[0];
+            a[v][2] = P(tri.vertex_ids[v], 1) - tri.ref_centroid[1];
+        }
+        la::inverse3(a, inv);
+        double* c = &coeffs[static_cast<size_t>(tri.id) * 24];
+        for (int v = 0; v < 3; ++v) {
+            c[v] = inv[1][v];
+            c[3 + v] = inv[2][v];
+        }
+        for (int n = 0; n < 6; ++n)
+            for (int k = 0; k < 3; ++k) c[6 + 3 * n + k] = tri.mat_for_patch_2nd_derivs[n][k];
+    }
+}
+
+// source_files/calc_dof_masses.cpp:45-58: a third of each triangle's mass to
+// each of its vertices (one value per node; x, y and z dofs are equal).
+void calc_dof_masses(std::vector<double>& m, const std::vector<Tri>& triangles, const Stuff& stuff) {
+    m.assign(stuff.num_nodes, 0.0);
+    for (const auto& tri : triangles)
+        for (int v = 0; v < 3; ++v) m[tri.vertex_ids[v]] += stuff.ref_density * tri.ref_area * tri.ref_thickness / 3.0;
+}
+
+// source_files/calc_char_mechanics_scales.cpp:45-73
+void calc_char_mechanics_scales(const std::vector<Tri>& triangles, Stuff& stuff) {
+    std::vector<double> h, mu, area;
+    for (const auto& t : triangles) {
+        h.push_back(t.ref_thickness);
+        mu.push_back(t.ref_shear_modulus);
+        area.push_back(t.ref_area);
+    }
+    stuff.min_ref_thickness = vmin(h);
+    stuff.min_ref_shear_modulus = vmin(mu);
+    stuff.char_flexural_rigidity = (1.0 / 6.0) * stuff.min_ref_shear_modulus * stuff.min_ref_thickness *
+                                   stuff.min_ref_thickness * stuff.min_ref_thickness / (1.0 - stuff.def_poisson_ratio);
+    stuff.char_force_scale = stuff.min_ref_shear_modulus * stuff.approx_min_tri_size * stuff.min_ref_thickness;
+    stuff.char_speed_scale = std::sqrt(stuff.min_ref_shear_modulus / stuff.ref_density);
+    stuff.char_stretch_energy_density_scale = stuff.min_ref_shear_modulus * stuff.min_ref_thickness;
+    stuff.char_stretch_energy_scale = stuff.char_stretch_energy_density_scale * kahan_sum(area);
+}
+
+// source_files/calc_long_timescales.cpp:40-61
+void calc_long_timescales(Stuff& stuff, Log& log) {
+    const double pi = 3.14159265358979323846;
+    const double k = 2.0 * pi / stuff.sample_char_length;
+    stuff.stretch_long_time = 2.0 * pi * std::sqrt(stuff.ref_density / stuff.min_ref_shear_modulus) / k;
+    stuff.bend_long_time =
+        2.0 * pi * std::sqrt(stuff.ref_density * stuff.min_ref_thickness / stuff.char_flexural_rigidity) / (k * k);
+    stuff.char_long_time = stuff.stretch_long_time > stuff.bend_long_time ? stuff.stretch_long_time : stuff.bend_long_time;
+    log << "The long characteristic time = " << stuff.char_long_time << std::endl;
+}
+
+// source_files/calc_damping_factor.cpp:42-58
+void calc_damping_factor(double prefactor, Stuff& stuff, Log& log) {
+    const double pi = 3.14159265358979323846;
+    const double k = 2.0 * pi / stuff.sample_char_length;
+    const double scale = 2.0 * std::sqrt(stuff.char_flexural_rigidity * stuff.ref_density * stuff.min_ref_thickness *
+                                         stuff.min_ref_thickness * stuff.min_ref_thickness) *
+                         k * k;
+    stuff.damping_factor = prefactor * scale;
+    log << "Numerical Damping Coefficient = " << stuff.damping_factor << std::endl;
+}
+
+// source_files/calc_timestep.cpp:41-73
+void calc_timestep(Stuff& stuff, Log& log) {
+    const double pi = 3.14159265358979323846;
+    double st = 0.185 * stuff.timestep_prefactor * std::sqrt(stuff.ref_density / stuff.min_ref_shear_modulus) *
+                stuff.approx_min_tri_size;
+    double bt = stuff.timestep_prefactor *
+                std::sqrt(stuff.ref_density * stuff.min_ref_thickness / stuff.char_flexural_rigidity) *
+                stuff.approx_min_tri_size * stuff.approx_min_tri_size / (2 * pi);
+    log << "Short stretching and bending timescales: " << st << ", " << bt << std::endl;
+    if (stuff.using_gradient_descent_dynamics) {
+        st = 0.185 * stuff.timestep_prefactor *
+             (stuff.damping_factor / (stuff.min_ref_shear_modulus * stuff.min_ref_thickness * stuff.min_ref_thickness)) *
+             stuff.approx_min_tri_size * stuff.approx_min_tri_size / (2.0 * pi);
+        bt = stuff.timestep_prefactor * (stuff.damping_factor / (stuff.char_flexural_rigidity * stuff.min_ref_thickness)) *
+             stuff.approx_min_tri_size * stuff.approx_min_tri_size * stuff.approx_min_tri_size *
+             stuff.approx_min_tri_size / (2.0 * pi * 2.0 * pi * 2.0 * pi);
+    }
+    if (st < bt) {
+        stuff.timestep = st;
+        log << "Time step = " << stuff.timestep << ", set based on stretching rather than bending." << std::endl;
+    } else {
+        stuff.timestep = bt;
+        log << "Time step = " << stuff.timestep << ", set based on bending rather than stretching." << std::endl;
+    }
+}
+
+// source_files/calc_steps_between_outputs.cpp:40-66
+void calc_steps_between_outputs(Stuff& stuff, Log& log) {
+    if (stuff.outputs_per_char_long_time < 0.0) {
+        stuff.steps_between_outputs = -1;
+        stuff.output_regularly = false;
+        log << "The setting printouts_per_char_long_time < 0, so regular printouts have been turned off completely."
+            << std::endl;
+    } else {
+        if (stuff.outputs_per_char_long_time < 1.0)
+            throw std::runtime_error(
+                "Error: To avoid potential divide-by-zero problems we do NOT allow stuff.printouts_per_char_long_time "
+                "to lie in [0.0, 1.0). This is overkill somewhat, and could be relaxed if need be.");
+        stuff.output_regularly = true;
+        stuff.steps_between_outputs =
+            std::lround(stuff.char_long_time / (stuff.timestep * stuff.outputs_per_char_long_time)) + 1;
+    }
+    if (stuff.using_gradient_descent_dynamics) stuff.steps_between_outputs = 1000;
+}
+
+// source_files/calc_dialling_procedure_params.cpp:52-80
+void calc_dialling_procedure_params(Stuff& stuff, Log& log) {
+    if (stuff.dial_factors_to_hold_at_spacing <= 0 || stuff.dial_phase_time_prefactor < 0)
+        throw std::runtime_error(
+            "\nstuff.step_between_dial_factors_to_hold_at and stuff.dial_phase_time must "
+            "be >0 and >=0 respectively, and they aren't currently. Aborting.");
+    stuff.dial_phase_time = stuff.dial_phase_time_prefactor * stuff.char_long_time;
+    stuff.timesteps_per_dial_phase = std::lround(stuff.dial_phase_time / stuff.timestep);
+    log << "Duration of each dialling phase = " << stuff.dial_phase_time << " which is "
+        << stuff.timesteps_per_dial_phase << " timesteps." << std::endl;
+    stuff.timesteps_between_equil_checks =
+        std::lround(stuff.time_between_equil_checks_prefactor * stuff.dial_phase_time / stuff.timestep);
+    if (stuff.timesteps_per_dial_phase <= 0)
+        throw std::runtime_error("Error: the dialling phase is shorter than one timestep.");
+}
+
+// source_files/perturb_node_positions_with_noise.cpp:45-62: uniform noise of
+// half-width 0.001 * approx_min_tri_size on every coordinate, from a
+// minimal-standard LCG seeded with 123456.
+void perturb_node_positions_with_noise(DMat& P, const Stuff& stuff) {
+    std::minstd_rand engine(123456);
+    std::uniform_real_distribution<double> distr(-stuff.approx_min_tri_size * 0.001, stuff.approx_min_tri_size * 0.001);
+    for (int n = 0; n < stuff.num_nodes; ++n)
+        for (int c = 0; c < 3; ++c) P(n, c) += distr(engine);
+}
+
+// source_files/initialize_glass_slides.cpp:27-48
+void initialize_glass_slides(const DMat& P, Stuff& stuff) {
+    if (stuff.using_initial_glass_slide_z_coords_from_settings_file) {
+        stuff.upper_slide_z_coord = stuff.initial_upper_slide_z_coord;
+        stuff.lower_slide_z_coord = stuff.initial_lower_slide_z_coord;
+    } else {
+        std::vector<double> z;
+        for (int n = 0; n < stuff.num_nodes; ++n) z.push_back(P(n, 2));
+        stuff.upper_slide_z_coord = vmax(z);
+        stuff.lower_slide_z_coord = vmin(z);
+    }
+}
+
+}  // namespace msb
