@@ -1,0 +1,356 @@
+"""Throughput of the force-and-dynamics loop: triangle-steps per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+                    [--workload disk1p8m] [--impl ours|reference]
+
+Workload (default ``disk1p8m``): unit disk, jittered hexagonal lattice of
+spacing 0.002 (908,139 nodes, 1,813,134 triangles), LCE dialling protocol 3
+with an azimuthal director perturbed by 0.3 sin(3 theta) and lambda dialled
+1 -> 0.85, bbar = 0, h = 0.01, nu = 0.5, unit modulus and density; seeded
+synthetic inputs (there is no public dataset for this path).  A step is one
+timestep of the dialling phase: surface derivatives, in-line dialling,
+deformation forces, damping, constraints, force guard and symplectic Euler
+update -- the fused GPU stepper launches two kernels per step.  Per-step
+traffic is ~1 GB, far above the 126 MB L2, so no flush is needed between
+steps.
+
+``value``: K * T * N / (max over ranks of the device time of K steps).
+``e2e``: the same metric with the state on the host, through the C ABI, every
+step: pinned host dofs + velocities copied in (ms_upload_dofs), one fused step
+(ms_step_n), dofs + velocities copied back (ms_download_dofs).
+Multi-GPU: one independent replica per GPU (the benchmark mesh fits one GPU);
+``scaling`` is weak.
+
+``--impl reference`` times the reference's own C++ (compiled from its source
+files against oracle/eigen_shim; the port oracle if that build is absent) on
+the host cores, with all threads, on the same mesh and metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# Algorithmic bytes per triangle-step of the timed variant (FP64, protocol-3
+# dialling evaluated in-kernel, bbar = 0): per triangle 6 int32 patch ids
+# (24 B), 24 derivative weights (192 B), 3 abar_info columns (24 B) and the
+# reference area (8 B); per node read+write of position and velocity
+# (96 B) and the mass (8 B), i.e. 104 B per node = 52 B per triangle at
+# N = T/2.  Mixed precision reads the 24 weights and the area as float.
+BYTES_PER_TRI = {"fp64": 24 + 192 + 24 + 8 + 52, "mixed": 24 + 96 + 24 + 4 + 52}
+METRIC = "tri-steps/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def make_workload(name: str, seed: int = 1):
+    from morphoshell_b200 import Model, meshgen
+    mesh, info, bbar = meshgen.workload(name, seed=seed)
+    d = tempfile.mkdtemp(prefix="ms_bench_")
+    st = os.path.join(d, "settings.txt")
+    meshgen.write_settings(st, protocol=3)
+    model = Model.from_arrays(st, mesh.nodes, mesh.tris, info, bbar)
+    return model, info, bbar
+
+
+def dial_sequence(model, n: int) -> np.ndarray:
+    s = model.scalars
+    k = np.arange(n, dtype=np.float64)
+    return 0.0 + s.dial_factors_to_hold_at_spacing * (k / float(s.timesteps_per_dial_phase))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(workload: str, precision: str):
+    """DRAM bytes per step from the committed ncu summary, if one exists."""
+    p = os.path.join(ROOT, "profiles", "step_traffic.txt")
+    try:
+        with open(p) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 3 and parts[0] == workload and parts[1] == precision:
+                    return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline(model, info, bbar, budget_s: float = 20.0):
+    """The reference's own CPU path on a bounded sample of this workload."""
+    import oracle
+    kind = "ref" if oracle.available("ref") else "orc"
+    cores = os.cpu_count() or 1
+    o = oracle.Oracle(kind, model, threads=cores)
+    s = model.scalars
+    o.set_programmed(3, info, bbar, s.dial_factors_to_hold_at_spacing)
+    o.upload(model.dofs(1))
+    dials = dial_sequence(model, 1000)
+    t0 = time.perf_counter()
+    o.step_n(1, dials[:1], s.timestep, s.damping_factor_1)
+    one = time.perf_counter() - t0
+    n = int(max(2, min(200, budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    o.step_n(n, dials[1:1 + n], s.timestep, s.damping_factor_1)
+    el = time.perf_counter() - t0
+    o.close()
+    return {"value": model.num_tris * n / el, "unit": METRIC, "cores": cores,
+            "kind": "reference" if kind == "ref" else "port",
+            "sample": "%d steps of the full %d-triangle mesh (protocol-3 dialling) after 1 warm-up step, %d threads"
+                      % (n, model.num_tris, cores)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    model, info, bbar = make_workload(args.workload)
+    kind = "ref" if oracle.available("ref") else "orc"
+    cores = os.cpu_count() or 1
+    o = oracle.Oracle(kind, model, threads=cores)
+    s = model.scalars
+    o.set_programmed(3, info, bbar, s.dial_factors_to_hold_at_spacing)
+    o.upload(model.dofs(1))
+    dials = dial_sequence(model, args.warmup + args.steps + 1)
+    # Warm-up (at most 2 steps: each is a full CPU step of the whole mesh),
+    # then as many of the K steps as fit in ~60 s of host time.
+    w = min(args.warmup, 2)
+    t0 = time.perf_counter()
+    o.step_n(w, dials[:w], s.timestep, s.damping_factor_1)
+    one = (time.perf_counter() - t0) / max(w, 1)
+    n = int(max(1, min(args.steps, 60.0 / max(one, 1e-9))))
+    t0 = time.perf_counter()
+    o.step_n(n, dials[w:w + n], s.timestep, s.damping_factor_1)
+    el = time.perf_counter() - t0
+    value = model.num_tris * n / el
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "impl": "reference", "n_gpus": args.gpus,
+        "steps": n, "warmup": w, "ms_per_step": 1e3 * el / n,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(args, model),
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores,
+                         "kind": "reference" if kind == "ref" else "port",
+                         "sample": "%d of the requested %d steps of the full mesh, %d threads"
+                                   % (n, args.steps, cores)},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(args, model):
+    return {"workload": "%s: unit disk, jittered hex spacing 0.002, %d nodes, %d triangles, LCE protocol-3 "
+                        "dialling (lambda 1 -> 0.85), bbar = 0, h = 0.01, nu = 0.5" % (
+                            args.workload, model.num_nodes, model.num_tris),
+            "precision": args.precision, "num_tris": model.num_tris, "num_nodes": model.num_nodes,
+            "l2": "inputs larger than L2 (~1 GB moved per step vs 126 MB L2); no flush",
+            "parallelism": "replicas x%d" % args.gpus}
+
+
+def run_ours(args):
+    import torch
+    from morphoshell_b200 import MS_PRECISION_FP64, MS_PRECISION_MIXED, GpuLoop, lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+
+    model, info, bbar = make_workload(args.workload)
+    s = model.scalars
+    T = model.num_tris
+    prec = MS_PRECISION_MIXED if args.precision == "mixed" else MS_PRECISION_FP64
+    g = GpuLoop(model, precision=prec, device=local)
+    g.set_programmed(3, info, bbar, s.dial_factors_to_hold_at_spacing)
+    g.upload(model.dofs(1))
+    dials = dial_sequence(model, args.warmup + args.steps + 64)
+    dt, damp = s.timestep, s.damping_factor_1
+
+    g.step_n(args.warmup, dials[:args.warmup], dt, damp)
+    stream = torch.cuda.ExternalStream(g.stream(), device=torch.device("cuda", local))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        g.step_n(args.steps, dials[args.warmup:args.warmup + args.steps], dt, damp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = T * args.steps * world / (ms_max / 1e3)
+
+    # Per-kernel device time for the roofline (CUDA events on the library's stream).
+    t_tri, t_node = g.time_kernels(50, dial=float(dials[args.warmup]), dt=dt, damping=damp)
+    step_ms = t_tri + t_node
+    bpt = BYTES_PER_TRI[args.precision]
+    achieved = bpt * T / (step_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    traffic = profiled_traffic(args.workload, args.precision)
+
+    # End to end through the C ABI with the state on the host every step.
+    N = model.num_nodes
+    hx = torch.empty(3 * N, dtype=torch.float64, pin_memory=True).numpy()
+    hv = torch.empty(3 * N, dtype=torch.float64, pin_memory=True).numpy()
+    g.download()
+    hx[:], hv[:] = g.download()
+    e2e_steps = min(args.steps, 200)
+    dl = dials[args.warmup:args.warmup + e2e_steps]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    L = lib()
+    import ctypes as C
+    pd = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    from morphoshell_b200 import ms_step_report
+    rep = ms_step_report()
+    for i in range(e2e_steps):
+        L.ms_upload_dofs(g._h, pd(hx), pd(hv))
+        one = np.ascontiguousarray(dl[i:i + 1])
+        L.ms_step_n(g._h, 1, pd(one), 1, dt, damp, 0, 0, C.byref(rep))
+        L.ms_download_dofs(g._h, pd(hx), pd(hv))
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e2.elapsed_time(e3)
+    t2 = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_value = T * e2e_steps * world / (float(t2.item()) / 1e3)
+
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed", "data": "synthetic",
+        "config": workload_config(args, model),
+        "gpu_launches": 2 * args.steps + (args.steps + 127) // 128,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "one step = k_tri_fused + k_node_update",
+                     "algorithmic_bytes_per_tri": bpt,
+                     "kernel_ms": {"k_tri_fused": t_tri, "k_node_update": t_node}},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 2 * 24 * N + 8,
+                "d2h_bytes_per_step": 2 * 24 * N + 16, "steps": e2e_steps},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(model, info, bbar)
+    g.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--workload", default="disk1p8m")
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -171,6 +171,16 @@ ms_status ms_output_quantities(ms_handle* h, double* curvatures, double* energy_
 /* Library and device description, for logs. */
 ms_status ms_device_info(char* buf, size_t len);
 
+/* The cudaStream_t the handle launches on (as void*), for callers that order
+ * or time their own work around it. */
+void* ms_stream(ms_handle* h);
+
+/* Mean device time of one launch of each fused-step kernel over `reps`
+ * steps (CUDA events on the handle's stream; the steps advance the state):
+ * the per-triangle kernel (ms_tri) and the per-node kernel (ms_node). */
+ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial_factor, double timestep,
+                          double damping_factor, double* ms_tri, double* ms_node);
+
 #ifdef __cplusplus
 }
 #endif

@@ -47,6 +47,15 @@ typedef struct msh_scalars {
 /* settings_path and vtk_path as the reference's command line; ansatz_path
  * may be NULL.  flags: bit 0 quiet (no stdout), bit 1 skip the initial noise. */
 int msh_load(const char* settings_path, const char* vtk_path, const char* ansatz_path, int flags, msh_model** out);
+/* Same set-up with the mesh handed over in memory instead of a VTK file
+ * (the CELL_DATA / POINT_DATA fields of read_vtk_data.cpp as arrays):
+ * positions N x 3, tri_vertex_ids T x 3, abar_info T x ka, bbar_info T x kb,
+ * all row-major; ref_thicknesses / ref_shear_moduli (T) may be NULL when the
+ * settings give uniform values; constrained (N) may be NULL. */
+int msh_build(const char* settings_path, int32_t num_nodes, int32_t num_tris, const double* positions,
+              const int32_t* tri_vertex_ids, const double* abar_info, int32_t ka, const double* bbar_info, int32_t kb,
+              const double* ref_thicknesses, const double* ref_shear_moduli, const uint8_t* constrained, int flags,
+              msh_model** out);
 void msh_free(msh_model* m);
 const char* msh_last_error(void);
 

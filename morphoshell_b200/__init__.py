@@ -26,10 +26,10 @@ GPU_SYMBOLS = [
     "ms_download_forces", "ms_set_programmed", "ms_set_zero_dial_state", "ms_do_dialling",
     "ms_download_programmed", "ms_surface_derivs", "ms_a_b_normals", "ms_deformation_forces",
     "ms_non_deformation_forces", "ms_impose_constraints", "ms_is_at_equilibrium", "ms_advance_dynamics",
-    "ms_step_n", "ms_output_quantities", "ms_device_info",
+    "ms_step_n", "ms_output_quantities", "ms_device_info", "ms_stream", "ms_time_kernels",
 ]
 HOST_SYMBOLS = [
-    "msh_load", "msh_free", "msh_last_error", "msh_get_scalars", "msh_get_desc", "msh_get_dofs",
+    "msh_load", "msh_build", "msh_free", "msh_last_error", "msh_get_scalars", "msh_get_desc", "msh_get_dofs",
     "msh_get_programmed", "msh_get_tri_vertices", "msh_get_boundary", "msh_run",
 ]
 
@@ -127,7 +127,12 @@ def lib() -> C.CDLL:
                                 P(ms_step_report)]
         L.ms_output_quantities.argtypes = [C.c_void_p, d, d, d, d, d, d]
         L.ms_device_info.argtypes = [C.c_char_p, C.c_size_t]
+        L.ms_stream.argtypes = [C.c_void_p]
+        L.ms_stream.restype = C.c_void_p
+        L.ms_time_kernels.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, d, d]
         L.msh_load.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, P(C.c_void_p)]
+        L.msh_build.argtypes = [C.c_char_p, C.c_int32, C.c_int32, d, P(C.c_int32), d, C.c_int32, d, C.c_int32,
+                                d, d, P(C.c_uint8), C.c_int, P(C.c_void_p)]
         L.msh_free.argtypes = [C.c_void_p]
         L.msh_free.restype = None
         L.msh_last_error.restype = C.c_char_p
@@ -153,15 +158,18 @@ def _f64(a):
 class Model:
     """Host set-up of one run (msh_load): settings + mesh (+ ansatz)."""
 
-    def __init__(self, settings_path: str, vtk_path: str, ansatz_path: str | None = None,
-                 quiet: bool = True, noise: bool = True):
+    def __init__(self, settings_path: str, vtk_path: str | None, ansatz_path: str | None = None,
+                 quiet: bool = True, noise: bool = True, _handle=None):
         L = lib()
-        h = C.c_void_p()
-        flags = (1 if quiet else 0) | (0 if noise else 2)
-        rc = L.msh_load(settings_path.encode(), vtk_path.encode(),
-                        ansatz_path.encode() if ansatz_path else None, flags, C.byref(h))
-        if rc != 0:
-            raise RuntimeError(L.msh_last_error().decode())
+        if _handle is None:
+            h = C.c_void_p()
+            flags = (1 if quiet else 0) | (0 if noise else 2)
+            rc = L.msh_load(settings_path.encode(), vtk_path.encode(),
+                            ansatz_path.encode() if ansatz_path else None, flags, C.byref(h))
+            if rc != 0:
+                raise RuntimeError(L.msh_last_error().decode())
+        else:
+            h = _handle
         self._h = h
         s = msh_scalars()
         L.msh_get_scalars(h, C.byref(s))
@@ -169,6 +177,29 @@ class Model:
         self.desc = ms_mesh_desc()
         self.params = ms_params()
         L.msh_get_desc(h, C.byref(self.desc), C.byref(self.params))
+
+    @classmethod
+    def from_arrays(cls, settings_path: str, positions, tris, abar_info, bbar_info, thickness=None,
+                    shear_modulus=None, constrained=None, quiet: bool = True, noise: bool = True) -> "Model":
+        """Set-up from in-memory mesh arrays (msh_build) instead of a VTK file."""
+        L = lib()
+        pos = np.ascontiguousarray(positions, dtype=np.float64)
+        if pos.shape[1] == 2:
+            pos = np.ascontiguousarray(np.column_stack([pos, np.zeros(len(pos))]))
+        tri = np.ascontiguousarray(tris, dtype=np.int32)
+        a = np.ascontiguousarray(abar_info, dtype=np.float64)
+        b = np.ascontiguousarray(bbar_info, dtype=np.float64)
+        th = None if thickness is None else np.ascontiguousarray(thickness, dtype=np.float64)
+        sm = None if shear_modulus is None else np.ascontiguousarray(shear_modulus, dtype=np.float64)
+        cn = None if constrained is None else np.ascontiguousarray(constrained, dtype=np.uint8)
+        h = C.c_void_p()
+        flags = (1 if quiet else 0) | (0 if noise else 2)
+        rc = L.msh_build(settings_path.encode(), pos.shape[0], tri.shape[0], _dp(pos),
+                         tri.ctypes.data_as(C.POINTER(C.c_int32)), _dp(a), a.shape[1], _dp(b), b.shape[1], _dp(th),
+                         _dp(sm), None if cn is None else cn.ctypes.data_as(C.POINTER(C.c_uint8)), flags, C.byref(h))
+        if rc != 0:
+            raise RuntimeError(L.msh_last_error().decode())
+        return cls(settings_path, None, _handle=h)
 
     def __del__(self):
         if getattr(self, "_h", None):
@@ -328,6 +359,17 @@ class GpuLoop:
             raise err
         self._chk(rc, "step_n")
         return rep
+
+    def stream(self) -> int:
+        """cudaStream_t of this handle, as an integer."""
+        return lib().ms_stream(self._h) or 0
+
+    def time_kernels(self, reps, dial=None, dt=0.0, damping=0.0):
+        """Mean device ms per launch of (per-triangle kernel, per-node kernel)."""
+        a, b = np.zeros(1), np.zeros(1)
+        self._chk(lib().ms_time_kernels(self._h, reps, 0 if dial is None else 1, 0.0 if dial is None else dial, dt,
+                                        damping, _dp(a), _dp(b)), "time_kernels")
+        return float(a[0]), float(b[0])
 
     def output_quantities(self):
         T, N = self.T, self.N

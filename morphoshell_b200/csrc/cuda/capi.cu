@@ -676,6 +676,60 @@ ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, doub
     return MS_OK;
 }
 
+void* ms_stream(ms_handle* h) { return h ? (void*)h->stream : nullptr; }
+
+ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial, double dt, double damping, double* ms_tri,
+                          double* ms_node) {
+    if (!h || reps <= 0 || !ms_tri || !ms_node) return MS_ERR_INVALID_ARGUMENT;
+    if (dialling && !h->programmed) return fail(h, MS_ERR_INVALID_ARGUMENT, "ms_set_programmed has not been called");
+    const bool fuse_lce = dialling && lce_fusable(h);
+    if (dialling && !fuse_lce) return fail(h, MS_ERR_UNSUPPORTED, "kernel timing covers the fused protocol-3 path");
+    cudaStream_t st = h->stream;
+    if (dialling) {
+        std::vector<double> d(reps, dial);
+        if (h->dials_cap < reps) {
+            if (h->d_dials) {
+                cudaFree(h->d_dials);
+                h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->d_dials), h->allocs.end());
+            }
+            MS_TRY(dalloc(h, &h->d_dials, std::max(reps, 1024)));
+            h->dials_cap = std::max(reps, 1024);
+            h->s.dials = h->d_dials;
+            clear_graphs(h);
+        }
+        MS_CUDA(h, cudaMemcpy(h->d_dials, d.data(), reps * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    MS_TRY(reset_error(h));
+    std::vector<cudaEvent_t> ev(3 * reps);
+    for (auto& e : ev) MS_CUDA(h, cudaEventCreate(&e));
+    int p = h->cur;
+    for (int i = 0; i < reps; ++i) {
+        StepScalars sc{i, p, dt, damping, h->rho_hh, h->force_limit, 0, 0};
+        MS_CUDA(h, cudaEventRecord(ev[3 * i], st));
+        MS_CUDA(h, launch_tri_fused(h->m, h->s, sc, fuse_lce ? DIAL_LCE : DIAL_ARRAYS, h->precision, st));
+        MS_CUDA(h, cudaEventRecord(ev[3 * i + 1], st));
+        MS_CUDA(h, launch_node_update(h->m, h->s, sc, h->precision, st));
+        MS_CUDA(h, cudaEventRecord(ev[3 * i + 2], st));
+        p ^= 1;
+    }
+    MS_CUDA(h, cudaStreamSynchronize(st));
+    double a = 0, b = 0;
+    for (int i = 0; i < reps; ++i) {
+        float t1 = 0, t2 = 0;
+        cudaEventElapsedTime(&t1, ev[3 * i], ev[3 * i + 1]);
+        cudaEventElapsedTime(&t2, ev[3 * i + 1], ev[3 * i + 2]);
+        a += t1;
+        b += t2;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    MS_CUDA(h, cudaMemcpy(h->h_err, h->s.err, sizeof(DevError), cudaMemcpyDeviceToHost));
+    if (h->h_err->flag) return fail(h, MS_ERR_IMPLAUSIBLE_FORCE, "implausibly_high_force during kernel timing");
+    h->cur = p;
+    *ms_tri = a / reps;
+    *ms_node = b / reps;
+    return MS_OK;
+}
+
 ms_status ms_output_quantities(ms_handle* h, double* curv, double* edens, double* strains, double* stresses,
                                double* deficits, double* energies) {
     if (!h) return MS_ERR_INVALID_ARGUMENT;

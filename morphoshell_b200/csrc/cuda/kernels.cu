@@ -490,7 +490,9 @@ __global__ void k_dialling(const DevMesh m, int protocol, double dial_in, double
     } else if (protocol == 4) {
         const double nu_ot = IA(11);
         const double angle = IA(12);
-        const int idx = (int)floor(dial / spacing);
+        // The reference reads columns idx and idx + 1 unchecked; keep both
+        // inside the table (the last checkpoint holds beyond its range).
+        const int idx = max(0, min((int)floor(dial / spacing), m.ka - 1));
         const double frac = dial / spacing - idx;
         const double prev = IA(idx);
         const double next = (idx + 1 < m.ka) ? IA(idx + 1) : prev;

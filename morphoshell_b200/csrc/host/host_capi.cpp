@@ -51,8 +51,63 @@ extern "C" {
 
 const char* msh_last_error(void) { return g_err.c_str(); }
 
-int msh_load(const char* settings_path, const char* vtk_path, const char* ansatz_path, int flags, msh_model** out) {
-    if (!settings_path || !vtk_path || !out) return set_err("null argument");
+}  // extern "C"
+
+namespace {
+
+// Mesh data handed over in memory instead of read from the input VTK file.
+struct ArrayMesh {
+    int N, T;
+    const double* pos;
+    const int32_t* tris;
+    const double* abar_info;
+    int ka;
+    const double* bbar_info;
+    int kb;
+    const double* thick;
+    const double* shear;
+    const uint8_t* constrained;
+};
+
+// Fills what read_vtk_data would (read_vtk_data.cpp:84-371), including the
+// uniform thickness / modulus overrides of the settings file.
+void fill_from_arrays(msh_model& m, const ArrayMesh& a) {
+    Stuff& st = m.stuff;
+    if (a.N <= 0 || a.T <= 0 || a.ka <= 0 || a.kb <= 0)
+        throw std::runtime_error("Error: mesh arrays have a non-positive size.");
+    st.num_nodes = a.N;
+    st.num_tris = a.T;
+    m.nodes.assign(a.N, Node());
+    m.ref_positions.resize(a.N, 3);
+    for (int n = 0; n < a.N; ++n) {
+        m.nodes[n].id = n;
+        m.nodes[n].is_constrained = a.constrained ? a.constrained[n] != 0 : false;
+        for (int c = 0; c < 3; ++c) m.ref_positions(n, c) = a.pos[3 * (size_t)n + c];
+    }
+    m.tris.assign(a.T, Tri());
+    bool found_zero = false;
+    for (int t = 0; t < a.T; ++t) {
+        m.tris[t].id = t;
+        for (int v = 0; v < 3; ++v) {
+            const int id = a.tris[3 * (size_t)t + v];
+            if (id < 0 || id >= a.N) throw std::runtime_error("Error: a triangle vertex id is out of range.");
+            found_zero |= id == 0;
+            m.tris[t].vertex_ids[v] = id;
+        }
+        m.tris[t].ref_thickness = st.ref_thickness_if_uniform > 0 ? st.ref_thickness_if_uniform : a.thick[t];
+        m.tris[t].ref_shear_modulus =
+            st.ref_shear_modulus_if_uniform > 0 ? st.ref_shear_modulus_if_uniform : a.shear[t];
+    }
+    if (!found_zero) throw std::runtime_error("Error: MorphoShell requires node ids starting from 0.");
+    m.abar_info.resize(a.T, a.ka);
+    std::memcpy(m.abar_info.v.data(), a.abar_info, sizeof(double) * (size_t)a.T * a.ka);
+    m.bbar_info.resize(a.T, a.kb);
+    std::memcpy(m.bbar_info.v.data(), a.bbar_info, sizeof(double) * (size_t)a.T * a.kb);
+}
+
+int load_common(const char* settings_path, const char* vtk_path, const ArrayMesh* arrays, const char* ansatz_path,
+                int flags, msh_model** out) {
+    if (!settings_path || (!vtk_path && !arrays) || !out) return set_err("null argument");
     *out = nullptr;
     auto m = std::make_unique<msh_model>();
     Stuff& st = m->stuff;
@@ -60,12 +115,17 @@ int msh_load(const char* settings_path, const char* vtk_path, const char* ansatz
     log.set_quiet(flags & 1);
     try {
         st.settings_filepath = settings_path;
-        st.ref_data_filepath = vtk_path;
+        st.ref_data_filepath = vtk_path ? vtk_path : "in-memory mesh";
         st.ansatz_file_was_given = ansatz_path != nullptr;
         st.ansatz_filepath = ansatz_path ? ansatz_path : "no_ansatz_file";
         read_settings(st, log);
-        read_vtk_data(m->nodes, m->ref_positions, m->ansatz, m->tris, m->abar_info, m->bbar_info, st,
-                      m->dial_factor_to_start_from, log);
+        if (arrays) {
+            if (st.ansatz_file_was_given) throw std::runtime_error("Error: in-memory meshes take no ansatz file.");
+            fill_from_arrays(*m, *arrays);
+        } else {
+            read_vtk_data(m->nodes, m->ref_positions, m->ansatz, m->tris, m->abar_info, m->bbar_info, st,
+                          m->dial_factor_to_start_from, log);
+        }
         if (st.dialling_from_ansatz_rather_than_ref_state) m->dial_factor_to_start_from = 0.0;
         calc_mesh_info(m->nodes, m->ref_positions, m->tris, m->edges, st, log);
         set_up_patch_fitting(m->nodes, m->ref_positions, m->tris, st, log);
@@ -111,6 +171,26 @@ int msh_load(const char* settings_path, const char* vtk_path, const char* ansatz
     }
     *out = m.release();
     return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int msh_load(const char* settings_path, const char* vtk_path, const char* ansatz_path, int flags, msh_model** out) {
+    return load_common(settings_path, vtk_path, nullptr, ansatz_path, flags, out);
+}
+
+int msh_build(const char* settings_path, int32_t num_nodes, int32_t num_tris, const double* positions,
+              const int32_t* tri_vertex_ids, const double* abar_info, int32_t ka, const double* bbar_info, int32_t kb,
+              const double* ref_thicknesses, const double* ref_shear_moduli, const uint8_t* constrained, int flags,
+              msh_model** out) {
+    if (!positions || !tri_vertex_ids || !abar_info || !bbar_info) return set_err("null argument");
+    std::vector<double> ones(num_tris > 0 ? num_tris : 0, 1.0);
+    ArrayMesh a{num_nodes, num_tris, positions, tri_vertex_ids, abar_info, ka, bbar_info, kb,
+                ref_thicknesses ? ref_thicknesses : ones.data(), ref_shear_moduli ? ref_shear_moduli : ones.data(),
+                constrained};
+    return load_common(settings_path, nullptr, &a, nullptr, flags, out);
 }
 
 void msh_free(msh_model* m) { delete m; }

@@ -292,7 +292,7 @@ void dialling(Ctx& c, double dial_in) {
                 break;
             case 4: {
                 const double nu_ot = A[11], angle = A[12];
-                const int idx = (int)std::floor(dial / c.spacing);
+                const int idx = std::max(0, std::min((int)std::floor(dial / c.spacing), c.ka - 1));
                 const double frac = dial / c.spacing - idx;
                 const double prev = A[idx];
                 const double next = idx + 1 < c.ka ? A[idx + 1] : prev;

@@ -18,7 +18,19 @@
 #include "Stuff_Class.hpp"
 #include "Tri_Class.hpp"
 #include "advance_dynamics.hpp"
+#include "Edge_Class.hpp"
 #include "calc_a_comps_and_b_comps_and_normals.hpp"
+#include "calc_char_mechanics_scales.hpp"
+#include "calc_damping_factor.hpp"
+#include "calc_dialling_procedure_params.hpp"
+#include "calc_long_timescales.hpp"
+#include "calc_mesh_info.hpp"
+#include "calc_steps_between_outputs.hpp"
+#include "calc_timestep.hpp"
+#include "perturb_node_positions_with_noise.hpp"
+#include "read_settings.hpp"
+#include "read_vtk_data.hpp"
+#include "set_up_patch_fitting.hpp"
 #include "calc_angle_deficits.hpp"
 #include "calc_curvatures.hpp"
 #include "calc_deformation_forces.hpp"
@@ -90,6 +102,82 @@ void dial(Ctx& c, double f) {
 extern "C" {
 
 void ref_set_threads(int n) { omp_set_num_threads(n); }
+
+// The reference's own set-up sequence (main.cpp:91-209): settings, mesh file,
+// topology, patch fitting, derivative matrix, masses, scales, timestep and
+// dialling schedule, initial noise.  Outputs (any may be NULL): patch T x 6,
+// mat2 T x 18, node masses N, initial dofs 3N (after noise), and
+// scal[14] = {sample_char_length, approx_min_tri_size, min_ref_thickness,
+// char_force_scale, char_speed_scale, char_long_time, damping_factor(pref 1),
+// timestep, timesteps_per_dial_phase, timesteps_between_equil_checks,
+// total_ref_area, num_edges, num_boundary_nodes, damping_factor(pref 2)}.
+// Returns 0, or 1 with the exception text in err (len bytes).
+int ref_setup_from_files(const char* settings, const char* vtk, int* N_out, int* T_out, int32_t* patch,
+                         double* mat2, double* masses, double* dofs0, double* scal, char* err, int len) {
+    try {
+        Stuff_Class st;
+        Out_Stream_Class log;
+        log.set_output_filepath("/dev/null");
+        st.settings_filepath = settings;
+        st.ref_data_filepath = vtk;
+        st.ansatz_file_was_given = false;
+        read_settings(st, log);
+        std::vector<Node_Class> nodes;
+        Eigen::Matrix<double, Eigen::Dynamic, 3> P;
+        std::vector<Eigen::Vector3d> ans;
+        std::vector<Tri_Class> tris;
+        MatXX ai, bi;
+        double d0 = 0.0;
+        read_vtk_data(nodes, P, ans, tris, ai, bi, st, d0, log);
+        std::vector<Edge_Class> edges;
+        calc_mesh_info(nodes, P, tris, edges, st, log);
+        set_up_patch_fitting(nodes, P, tris, st, log);
+        Sparse D(st.num_continuum_quantities, st.num_dofs), DT(st.num_dofs, st.num_continuum_quantities);
+        calc_deriv_mats(D, DT, P, tris, st, log);
+        VecX m(st.num_dofs, 1);
+        calc_dof_masses(m, tris, st, log);
+        calc_char_mechanics_scales(tris, st);
+        calc_long_timescales(st, log);
+        calc_damping_factor(st.damping_prefactor_2, st, log);
+        const double damp2 = st.damping_factor;
+        calc_damping_factor(st.damping_prefactor_1, st, log);
+        calc_timestep(st, log);
+        calc_steps_between_outputs(st, log);
+        calc_dialling_procedure_params(st, log);
+        perturb_node_positions_with_noise(P, st);
+        if (N_out) *N_out = st.num_nodes;
+        if (T_out) *T_out = st.num_tris;
+        for (int t = 0; t < st.num_tris; ++t) {
+            for (int v = 0; v < 3; ++v) {
+                if (patch) patch[6 * (size_t)t + v] = tris[t].vertex_ids[v];
+                if (patch) patch[6 * (size_t)t + 3 + v] = tris[t].non_vertex_patch_nodes_ids[v];
+            }
+            for (int r = 0; r < 6; ++r)
+                for (int k = 0; k < 3; ++k)
+                    if (mat2) mat2[18 * (size_t)t + 3 * r + k] = tris[t].mat_for_patch_2nd_derivs(r, k);
+        }
+        for (int n = 0; n < st.num_nodes; ++n) {
+            if (masses) masses[n] = m(n);
+            for (int k = 0; k < 3; ++k)
+                if (dofs0) dofs0[(size_t)k * st.num_nodes + n] = P(n, k);
+        }
+        if (scal) {
+            const double v[14] = {st.sample_char_length, st.approx_min_tri_size, st.min_ref_thickness,
+                                  st.char_force_scale, st.char_speed_scale, st.char_long_time, st.damping_factor,
+                                  st.timestep, (double)st.timesteps_per_dial_phase,
+                                  (double)st.timesteps_between_equil_checks, st.total_ref_area, (double)st.num_edges,
+                                  (double)st.num_boundary_nodes, damp2};
+            for (int k = 0; k < 14; ++k) scal[k] = v[k];
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        if (err && len > 0) {
+            std::strncpy(err, e.what(), len - 1);
+            err[len - 1] = 0;
+        }
+        return 1;
+    }
+}
 
 void* ref_create(int N, int T, const double* ref_pos, const int32_t* patch, const double* mat2, const double*,
                  const double*, const double* area, const double* thick, const double* shear, const uint8_t* fixed,
