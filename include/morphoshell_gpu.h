@@ -147,6 +147,31 @@ ms_status ms_is_at_equilibrium(ms_handle* h, ms_equil_result* out);
 ms_status ms_advance_dynamics(ms_handle* h, double timestep, double damping_factor, int using_gradient_descent,
                               int64_t* offending_dof, double* offending_force);
 
+/* Deformation forces (forces = -D^T dE/dcq, as ms_deformation_forces) for
+ * callers that cannot allocate device memory: code running while a CUDA
+ * graph is captured around it, host frameworks that route every device
+ * allocation through their own pool, real-time loops that must not allocate
+ * after start-up.  No counterpart in the reference (which never touches a
+ * GPU).  No handle is needed and nothing is allocated: every pointer is a
+ * DEVICE pointer the caller owns -- patch_ids 6T, deriv_coeffs 24T, ref_area,
+ * ref_thickness, ref_shear_modulus T, abar and bbar 3T (all in the
+ * ms_mesh_desc / row-major layouts above), dofs and forces 3N SoA.  Work
+ * space is a static device array inside this library, sized for at most
+ * 65,536 nodes and 65,536 triangles (about 11.5 MB that every GPU loading
+ * the library keeps until exit); larger meshes return
+ * MS_ERR_INVALID_ARGUMENT with the reason in err.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  All calls share the array:
+ * calls that overlap on the GPU race, so serialise them.  Runs on `stream`
+ * (a cudaStream_t, NULL for the default stream) and returns after the forces
+ * are written.  err (err_len bytes, may be NULL) receives a message. */
+ms_status ms_deformation_forces_noalloc(int32_t num_nodes, int32_t num_tris, const int32_t* patch_ids,
+                                        const double* deriv_coeffs, const double* ref_area,
+                                        const double* ref_thickness, const double* ref_shear_modulus,
+                                        const double* abar, const double* bbar, double def_poisson_ratio,
+                                        double bend_stiffening_scale_factor, const double* dofs, double* forces,
+                                        void* stream, char* err, size_t err_len);
+
 /* ---- fused stepper: the whole main.cpp:308-488 body per step ----------
  * Runs n steps of: surface derivs -> (dialling) -> deformation forces ->
  * damping -> constraints -> (equilibrium check on the last step if

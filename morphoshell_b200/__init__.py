@@ -27,6 +27,7 @@ GPU_SYMBOLS = [
     "ms_download_programmed", "ms_surface_derivs", "ms_a_b_normals", "ms_deformation_forces",
     "ms_non_deformation_forces", "ms_impose_constraints", "ms_is_at_equilibrium", "ms_advance_dynamics",
     "ms_step_n", "ms_output_quantities", "ms_device_info", "ms_stream", "ms_time_kernels",
+    "ms_deformation_forces_noalloc",
 ]
 HOST_SYMBOLS = [
     "msh_load", "msh_build", "msh_free", "msh_last_error", "msh_get_scalars", "msh_get_desc", "msh_get_dofs",
@@ -127,6 +128,10 @@ def lib() -> C.CDLL:
                                 P(ms_step_report)]
         L.ms_output_quantities.argtypes = [C.c_void_p, d, d, d, d, d, d]
         L.ms_device_info.argtypes = [C.c_char_p, C.c_size_t]
+        L.ms_deformation_forces_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                                    C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p,
+                                                    C.c_size_t]
         L.ms_stream.argtypes = [C.c_void_p]
         L.ms_stream.restype = C.c_void_p
         L.ms_time_kernels.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, d, d]
