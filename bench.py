@@ -218,7 +218,7 @@ def workload_config(args, model):
     return {"workload": "%s: unit disk, jittered hex spacing 0.002, %d nodes, %d triangles, LCE protocol-3 "
                         "dialling (lambda 1 -> 0.85), bbar = 0, h = 0.01, nu = 0.5" % (
                             args.workload, model.num_nodes, model.num_tris),
-            "precision": args.precision, "num_tris": model.num_tris, "num_nodes": model.num_nodes,
+            "precision": args.precision, "path": args.path, "num_tris": model.num_tris, "num_nodes": model.num_nodes,
             "l2": "inputs larger than L2 (~1 GB moved per step vs 126 MB L2); no flush",
             "parallelism": "replicas x%d" % args.gpus}
 
@@ -243,6 +243,8 @@ def run_ours(args):
     T = model.num_tris
     prec = MS_PRECISION_MIXED if args.precision == "mixed" else MS_PRECISION_FP64
     g = GpuLoop(model, precision=prec, device=local)
+    g.set_step_path(0 if args.path == "cluster" else 1)
+    plan = g.plan_info()
     g.set_programmed(3, info, bbar, s.dial_factors_to_hold_at_spacing)
     g.upload(model.dofs(1))
     dials = dial_sequence(model, args.warmup + args.steps + 64)
@@ -318,9 +320,12 @@ def run_ours(args):
         "gpu_launches": 2 * args.steps + (args.steps + 127) // 128,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "one step = k_tri_fused + k_node_update",
+                     "kernel": ("one step = k_cluster_step + k_halo_update" if args.path == "cluster"
+                                else "one step = k_tri_fused + k_node_update"),
                      "algorithmic_bytes_per_tri": bpt,
-                     "kernel_ms": {"k_tri_fused": t_tri, "k_node_update": t_node}},
+                     "kernel_ms": ({"k_cluster_step": t_tri, "k_halo_update": t_node} if args.path == "cluster"
+                                   else {"k_tri_fused": t_tri, "k_node_update": t_node})},
+        "plan": plan,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 2 * 24 * N + 8,
                 "d2h_bytes_per_step": 2 * 24 * N + 16, "steps": e2e_steps},
         "clocks": clocks,
@@ -345,6 +350,8 @@ def main():
     ap.add_argument("--workload", default="disk1p8m")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--path", choices=["cluster", "two-kernel"], default="cluster",
+                    help="fused-step implementation (ms_set_step_path)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -200,6 +200,19 @@ ms_status ms_device_info(char* buf, size_t len);
  * or time their own work around it. */
 void* ms_stream(ms_handle* h);
 
+/* Which implementation ms_step_n uses: 0 (default) the cluster-tiled step --
+ * each thread-block cluster owns a Morton tile of triangles, keeps their
+ * force contributions in distributed shared memory and updates the tile's
+ * interior nodes itself; 1 the two-kernel step (per-triangle kernel writes
+ * all contributions to HBM, per-node kernel gathers them).  Both sum every
+ * node's contributions in ascending triangle order. */
+ms_status ms_set_step_path(ms_handle* h, int path);
+/* Tiling of the cluster path: CTAs per cluster, triangles per CTA, number of
+ * clusters, number of halo nodes (summed by the second kernel), and the
+ * path in use. */
+ms_status ms_plan_info(ms_handle* h, int* cluster_size, int* tris_per_cta, int* clusters, int* halo_nodes,
+                       int* path);
+
 /* Mean device time of one launch of each fused-step kernel over `reps`
  * steps (CUDA events on the handle's stream; the steps advance the state):
  * the per-triangle kernel (ms_tri) and the per-node kernel (ms_node). */

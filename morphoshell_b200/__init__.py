@@ -27,7 +27,7 @@ GPU_SYMBOLS = [
     "ms_download_programmed", "ms_surface_derivs", "ms_a_b_normals", "ms_deformation_forces",
     "ms_non_deformation_forces", "ms_impose_constraints", "ms_is_at_equilibrium", "ms_advance_dynamics",
     "ms_step_n", "ms_output_quantities", "ms_device_info", "ms_stream", "ms_time_kernels",
-    "ms_deformation_forces_noalloc",
+    "ms_deformation_forces_noalloc", "ms_set_step_path", "ms_plan_info",
 ]
 HOST_SYMBOLS = [
     "msh_load", "msh_build", "msh_free", "msh_last_error", "msh_get_scalars", "msh_get_desc", "msh_get_dofs",
@@ -132,6 +132,9 @@ def lib() -> C.CDLL:
                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                                     C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p,
                                                     C.c_size_t]
+        L.ms_set_step_path.argtypes = [C.c_void_p, C.c_int]
+        ip = C.POINTER(C.c_int)
+        L.ms_plan_info.argtypes = [C.c_void_p, ip, ip, ip, ip, ip]
         L.ms_stream.argtypes = [C.c_void_p]
         L.ms_stream.restype = C.c_void_p
         L.ms_time_kernels.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, d, d]
@@ -364,6 +367,15 @@ class GpuLoop:
             raise err
         self._chk(rc, "step_n")
         return rep
+
+    def set_step_path(self, path: int):
+        """0: cluster-tiled step (default), 1: two-kernel step."""
+        self._chk(lib().ms_set_step_path(self._h, path), "set_step_path")
+
+    def plan_info(self) -> dict:
+        v = [C.c_int() for _ in range(5)]
+        self._chk(lib().ms_plan_info(self._h, *[C.byref(x) for x in v]), "plan_info")
+        return dict(zip(["cluster_size", "tris_per_cta", "clusters", "halo_nodes", "path"], [x.value for x in v]))
 
     def stream(self) -> int:
         """cudaStream_t of this handle, as an integer."""

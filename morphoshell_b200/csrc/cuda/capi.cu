@@ -2,6 +2,7 @@
 // memory ownership, the one-call-per-reference-function path, the fused
 // stepper captured in CUDA graphs, and the output diagnostics.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -66,6 +67,14 @@ struct ms_handle {
     std::vector<GraphEntry> graphs;
     long long use_clock = 0;
     std::string last_error;
+    // cluster-tiled step
+    ClusterPlan plan{};
+    bool have_plan = false;
+    bool have_cluster = false;
+    int step_path = 1;  // 0 cluster-tiled, 1 two-kernel (default: measured faster)
+    std::vector<double> area_host;
+    double lce_lam_final = 0, lce_nu = 0;
+    int halo_parts = 0;
 };
 
 namespace {
@@ -150,6 +159,146 @@ ms_status ensure_out(ms_handle* h, size_t bytes) {
 }
 
 bool lce_fusable(const ms_handle* h) { return h->protocol == 3 && !h->from_ansatz && h->precision >= 0; }
+
+template <typename T>
+ms_status upload(ms_handle* h, T** dst, const std::vector<T>& src) {
+    MS_TRY(dalloc(h, dst, src.size()));
+    if (!src.empty()) MS_CUDA(h, cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return MS_OK;
+}
+
+// Tiles of cs * tpc consecutive triangles, one per thread-block cluster; a
+// node is owned by a tile when all its incidences lie in it (see
+// ClusterPlan).  Falls back to the two-kernel step when cluster launches are
+// unavailable.
+ms_status build_cluster_plan(ms_handle* h, const ms_mesh_desc* d, const std::vector<int>& off,
+                             const std::vector<int>& ent) {
+    const int N = d->num_nodes, T = d->num_tris;
+    const int tpc = 768;
+    // The per-triangle tables below serve both paths; the tiling only the
+    // cluster path, which needs cluster launches.
+    h->have_cluster = prepare_cluster_kernels(tpc) == cudaSuccess;
+    cudaGetLastError();
+    const int cs = h->have_cluster ? choose_cluster_size(tpc, cluster_threads(), h->precision) : 1;
+    ClusterPlan& p = h->plan;
+    p.cs = cs;
+    p.tpc = tpc;
+    p.threads = cluster_threads();
+    const int ct = cs * tpc;
+    p.nclusters = (T + ct - 1) / ct;
+    std::vector<int> owner(N, -1);
+    for (int n = 0; n < N; ++n) {
+        if (off[n] == off[n + 1]) continue;
+        const int c0 = (ent[off[n]] / 6) / ct, c1 = (ent[off[n + 1] - 1] / 6) / ct;
+        if (c0 == c1) owner[n] = c0;
+    }
+    std::vector<int> own_base(p.nclusters + 1, 0), own_nodes, own_off, halo_nodes;
+    std::vector<unsigned short> own_ent;
+    for (int n = 0; n < N; ++n)
+        if (owner[n] >= 0) own_base[owner[n] + 1] += 1;
+    for (int c = 0; c < p.nclusters; ++c) own_base[c + 1] += own_base[c];
+    own_nodes.assign(own_base[p.nclusters], 0);
+    {
+        std::vector<int> fill(own_base.begin(), own_base.end() - 1);
+        for (int n = 0; n < N; ++n)
+            if (owner[n] >= 0) own_nodes[fill[owner[n]]++] = n;
+            else halo_nodes.push_back(n);
+    }
+    own_off.reserve(own_nodes.size() + 1);
+    own_off.push_back(0);
+    std::vector<int32_t> idx(8ULL * T, 0);
+    for (int t = 0; t < T; ++t)
+        for (int k = 0; k < 6; ++k) idx[8ULL * t + k] = d->patch_ids[6ULL * t + k];
+    for (size_t i = 0; i < own_nodes.size(); ++i) {
+        const int n = own_nodes[i], c = owner[n];
+        for (int k = off[n]; k < off[n + 1]; ++k) {
+            const int t = ent[k] / 6, slot = ent[k] % 6;
+            const int lt = t - c * ct, rank = lt / tpc, li = lt % tpc;
+            own_ent.push_back((unsigned short)((rank << 13) | (li << 3) | slot));
+        }
+        own_off.push_back((int)own_ent.size());
+    }
+    for (int n : halo_nodes)
+        for (int k = off[n]; k < off[n + 1]; ++k) idx[8ULL * (ent[k] / 6) + 6] |= 1 << (ent[k] % 6);
+    int4* tri_idx;
+    double* coef_aos;
+    int *d_own_base, *d_own_nodes, *d_own_off, *d_halo;
+    unsigned short* d_own_ent;
+    MS_TRY(dalloc(h, &tri_idx, 2ULL * T));
+    MS_CUDA(h, cudaMemcpy(tri_idx, idx.data(), idx.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    MS_TRY(dalloc(h, &coef_aos, 24ULL * T));
+    MS_CUDA(h, cudaMemcpy(coef_aos, d->deriv_coeffs, 24ULL * T * sizeof(double), cudaMemcpyHostToDevice));
+    if (h->precision == MS_PRECISION_MIXED) {
+        std::vector<float> cf(24ULL * T);
+        for (size_t k = 0; k < cf.size(); ++k) cf[k] = (float)d->deriv_coeffs[k];
+        float* coef_f;
+        MS_TRY(upload(h, &coef_f, cf));
+        p.coef_aos_f = coef_f;
+    }
+    MS_TRY(upload(h, &d_own_base, own_base));
+    MS_TRY(upload(h, &d_own_nodes, own_nodes));
+    MS_TRY(upload(h, &d_own_off, own_off));
+    MS_TRY(upload(h, &d_own_ent, own_ent));
+    MS_TRY(upload(h, &d_halo, halo_nodes));
+    p.tri_idx = tri_idx;
+    p.coef_aos = coef_aos;
+    p.own_base = d_own_base;
+    p.own_nodes = d_own_nodes;
+    p.own_off = d_own_off;
+    p.own_ent = d_own_ent;
+    p.halo_nodes = d_halo;
+    p.n_halo = (int)halo_nodes.size();
+    // Equilibrium partials: one per cluster-kernel CTA plus one per halo block.
+    h->halo_parts = p.n_halo > 0 ? (p.n_halo + 255) / 256 : 1;
+    const int parts = p.nclusters * p.cs + h->halo_parts;
+    if (parts > h->s.eq_blocks) {
+        EqPartial* ep;
+        MS_TRY(dalloc(h, &ep, parts));
+        h->s.eq_part = ep;
+        h->s.eq_blocks = parts;
+    }
+    h->have_plan = true;
+    return MS_OK;
+}
+
+// Per-triangle director trigonometry for the cluster kernel's protocol-3
+// dialling, and whether lambda_final and nu_ot are uniform (then lambda and
+// lambda^(-2 nu) are per-step scalars computed on the host).
+ms_status prepare_lce_tables(ms_handle* h, const double* info, int ka) {
+    if (!h->have_plan || h->protocol != 3 || ka < 3) return MS_OK;
+    const int T = h->m.T;
+    std::vector<double> aux(4ULL * T), ln(2ULL * T);
+    bool uniform = true;
+    for (int t = 0; t < T; ++t) {
+        const double ang = info[(size_t)t * ka], c = std::cos(ang), s = std::sin(ang);
+        aux[4ULL * t] = h->area_host[t];
+        aux[4ULL * t + 1] = c * c;
+        aux[4ULL * t + 2] = s * s;
+        aux[4ULL * t + 3] = c * s;
+        ln[2ULL * t] = info[(size_t)t * ka + 1];
+        ln[2ULL * t + 1] = info[(size_t)t * ka + 2];
+        uniform = uniform && ln[2ULL * t] == ln[0] && ln[2ULL * t + 1] == ln[1];
+    }
+    double4* d_aux;
+    double2* d_ln;
+    MS_TRY(dalloc(h, &d_aux, T));
+    MS_CUDA(h, cudaMemcpy(d_aux, aux.data(), aux.size() * sizeof(double), cudaMemcpyHostToDevice));
+    MS_TRY(dalloc(h, &d_ln, T));
+    MS_CUDA(h, cudaMemcpy(d_ln, ln.data(), ln.size() * sizeof(double), cudaMemcpyHostToDevice));
+    h->plan.tri_aux = d_aux;
+    h->plan.lce_ln = d_ln;
+    h->plan.lce_uniform = uniform ? 1 : 0;
+    h->lce_lam_final = ln[0];
+    h->lce_nu = ln[1];
+    return MS_OK;
+}
+
+bool use_cluster(const ms_handle* h, bool dialling) {
+    if (!h->have_plan || !h->have_cluster || h->step_path != 0) return false;
+    if (dialling && !lce_fusable(h)) return false;
+    if (dialling && !h->plan.tri_aux) return false;
+    return true;
+}
 
 }  // namespace
 
@@ -267,8 +416,8 @@ ms_status ms_create(const ms_mesh_desc* d, const ms_params* prm, int device, int
     m.mu_uniform = d->ref_shear_modulus[0];
 
     // Incidence lists: node -> (6t + slot), ascending t.
+    std::vector<int> off(N + 1, 0), ent(6ULL * T);
     {
-        std::vector<int> off(N + 1, 0), ent(6ULL * T);
         for (long long k = 0; k < 6LL * T; ++k) off[d->patch_ids[k] + 1] += 1;
         for (int n = 0; n < N; ++n) off[n + 1] += off[n];
         std::vector<int> fill(off.begin(), off.end() - 1);
@@ -336,6 +485,8 @@ ms_status ms_create(const ms_mesh_desc* d, const ms_params* prm, int device, int
         m.area_f = area_f;
         m.contrib_f = contrib_f;
     }
+    h->area_host.assign(d->ref_area, d->ref_area + T);
+    if ((st = build_cluster_plan(h, d, off, ent))) return bail(st);
     if (cudaMallocHost(&h->h_err, sizeof(DevError)) != cudaSuccess ||
         cudaMallocHost(&h->h_equil, sizeof(DevEquil)) != cudaSuccess)
         return bail(MS_ERR_CUDA);
@@ -421,6 +572,7 @@ ms_status ms_set_programmed(ms_handle* h, int protocol, const double* abar_info,
     h->from_ansatz = from_ansatz ? 1 : 0;
     h->programmed = true;
     clear_graphs(h);  // graphs bake the mesh struct
+    MS_TRY(prepare_lce_tables(h, abar_info, ka));
     return MS_OK;
 }
 
@@ -541,6 +693,59 @@ ms_status ms_advance_dynamics(ms_handle* h, double dt, double damping, int gd, i
     return MS_OK;
 }
 
+// Per-step {dial, lambda, lambda^(-2 nu)} triples for the device (the last two
+// are used when lambda_final and nu_ot are uniform; formed as do_dialling.cpp:116-118
+// forms them, in double on the host).
+static ms_status stage_dials(ms_handle* h, const double* dials, int n) {
+    if (h->dials_cap < 3 * n) {
+        if (h->d_dials) {
+            cudaFree(h->d_dials);
+            h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->d_dials), h->allocs.end());
+        }
+        const int cap = std::max(3 * n, 3072);
+        MS_TRY(dalloc(h, &h->d_dials, cap));
+        h->dials_cap = cap;
+        h->s.dials = h->d_dials;
+        clear_graphs(h);
+    }
+    if (h->h_dials_cap < 3 * n) {
+        if (h->h_dials) cudaFreeHost(h->h_dials);
+        const int cap = std::max(3 * n, 3072);
+        MS_CUDA(h, cudaMallocHost(&h->h_dials, cap * sizeof(double)));
+        h->h_dials_cap = cap;
+    }
+    MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (int i = 0; i < n; ++i) {
+        const double dial = dials[i];
+        const double lam = (1.0 - dial) * 1.0 + dial * h->lce_lam_final;
+        h->h_dials[3 * i] = dial;
+        h->h_dials[3 * i + 1] = lam;
+        h->h_dials[3 * i + 2] = std::pow(lam, -2.0 * h->lce_nu);
+    }
+    MS_CUDA(h, cudaMemcpyAsync(h->d_dials, h->h_dials, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    return MS_OK;
+}
+
+// The two kernels of one fused step on the selected path.
+static cudaError_t launch_step(ms_handle* h, const StepScalars& sc, bool cluster, int dial_mode, cudaStream_t st) {
+    cudaError_t e;
+    if (cluster) {
+        e = launch_cluster_step(h->m, h->plan, h->s, sc, dial_mode, h->precision, st);
+        if (e == cudaSuccess) e = launch_halo_update(h->m, h->plan, h->s, sc, h->precision, st);
+    } else {
+        e = launch_tri_aos(h->m, h->plan, h->s, sc, dial_mode, h->precision, st);
+        if (e == cudaSuccess) e = launch_node_update(h->m, h->s, sc, h->precision, st);
+    }
+    return e;
+}
+
+ms_status ms_set_step_path(ms_handle* h, int path) {
+    if (!h || path < 0 || path > 1) return MS_ERR_INVALID_ARGUMENT;
+    if (path == 0 && !h->have_cluster) return fail(h, MS_ERR_UNSUPPORTED, "cluster launches are unavailable");
+    h->step_path = path;
+    return MS_OK;
+}
+
 ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, double dt, double damping, int gd,
                     int check_last, ms_step_report* rep) {
     if (!h || n < 0) return MS_ERR_INVALID_ARGUMENT;
@@ -554,37 +759,17 @@ ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, doub
         return fail(h, MS_ERR_INVALID_ARGUMENT, "dialling steps need dial factors and ms_set_programmed");
     const bool fuse_lce = dialling && lce_fusable(h);
     const int dial_mode = fuse_lce ? DIAL_LCE : DIAL_ARRAYS;
+    const bool cluster = use_cluster(h, dialling != 0);
     cudaStream_t st = h->stream;
-
-    if (dialling) {
-        if (h->dials_cap < n) {
-            if (h->d_dials) {
-                cudaFree(h->d_dials);
-                h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->d_dials), h->allocs.end());
-            }
-            int cap = std::max(n, 1024);
-            MS_TRY(dalloc(h, &h->d_dials, cap));
-            h->dials_cap = cap;
-            h->s.dials = h->d_dials;
-            clear_graphs(h);
-        }
-        if (h->h_dials_cap < n) {
-            if (h->h_dials) cudaFreeHost(h->h_dials);
-            int cap = std::max(n, 1024);
-            MS_CUDA(h, cudaMallocHost(&h->h_dials, cap * sizeof(double)));
-            h->h_dials_cap = cap;
-        }
-        MS_CUDA(h, cudaStreamSynchronize(st));
-        std::memcpy(h->h_dials, dials, n * sizeof(double));
-        MS_CUDA(h, cudaMemcpyAsync(h->d_dials, h->h_dials, n * sizeof(double), cudaMemcpyHostToDevice, st));
-    }
+    if (dialling) MS_TRY(stage_dials(h, dials, n));
     MS_TRY(reset_error(h));
     const int p0 = h->cur;
     int done = 0;
     while (done < n) {
         const int len = std::min(kChunk, n - done);
         const bool last_chunk = done + len == n;
-        GraphKey key{len, p0 ^ (done & 1), dial_mode, gd, (check_last && last_chunk) ? 1 : 0, dt, damping};
+        GraphKey key{len, p0 ^ (done & 1), dial_mode + (cluster ? 16 : 0), gd, (check_last && last_chunk) ? 1 : 0,
+                     dt, damping};
         cudaGraphExec_t exec = nullptr;
         if (!(dialling && !fuse_lce))
             for (auto& g : h->graphs)
@@ -601,8 +786,7 @@ ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, doub
                     MS_CUDA(h, launch_dialling(h->m, h->protocol, dials[done + i], h->spacing, h->from_ansatz, st));
                     StepScalars sc{i, key.parity ^ (i & 1), dt, damping, h->rho_hh, h->force_limit, gd,
                                    (key.check_last && i == len - 1) ? 1 : 0};
-                    MS_CUDA(h, launch_tri_fused(h->m, h->s, sc, DIAL_ARRAYS, h->precision, st));
-                    MS_CUDA(h, launch_node_update(h->m, h->s, sc, h->precision, st));
+                    MS_CUDA(h, launch_step(h, sc, cluster, DIAL_ARRAYS, st));
                 }
                 MS_CUDA(h, launch_chunk_end(h->s, len, st));
                 done += len;
@@ -614,8 +798,7 @@ ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, doub
             for (int i = 0; i < len && ce == cudaSuccess; ++i) {
                 StepScalars sc{i, key.parity ^ (i & 1), dt, damping, h->rho_hh, h->force_limit, gd,
                                (key.check_last && i == len - 1) ? 1 : 0};
-                ce = launch_tri_fused(h->m, h->s, sc, dial_mode, h->precision, st);
-                if (ce == cudaSuccess) ce = launch_node_update(h->m, h->s, sc, h->precision, st);
+                ce = launch_step(h, sc, cluster, dial_mode, st);
             }
             if (ce == cudaSuccess) ce = launch_chunk_end(h->s, len, st);
             cudaError_t ee = cudaStreamEndCapture(st, &graph);
@@ -684,20 +867,11 @@ ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial, dou
     if (dialling && !h->programmed) return fail(h, MS_ERR_INVALID_ARGUMENT, "ms_set_programmed has not been called");
     const bool fuse_lce = dialling && lce_fusable(h);
     if (dialling && !fuse_lce) return fail(h, MS_ERR_UNSUPPORTED, "kernel timing covers the fused protocol-3 path");
+    const bool cluster = use_cluster(h, dialling != 0);
     cudaStream_t st = h->stream;
     if (dialling) {
         std::vector<double> d(reps, dial);
-        if (h->dials_cap < reps) {
-            if (h->d_dials) {
-                cudaFree(h->d_dials);
-                h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), (void*)h->d_dials), h->allocs.end());
-            }
-            MS_TRY(dalloc(h, &h->d_dials, std::max(reps, 1024)));
-            h->dials_cap = std::max(reps, 1024);
-            h->s.dials = h->d_dials;
-            clear_graphs(h);
-        }
-        MS_CUDA(h, cudaMemcpy(h->d_dials, d.data(), reps * sizeof(double), cudaMemcpyHostToDevice));
+        MS_TRY(stage_dials(h, d.data(), reps));
     }
     MS_TRY(reset_error(h));
     std::vector<cudaEvent_t> ev(3 * reps);
@@ -705,10 +879,13 @@ ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial, dou
     int p = h->cur;
     for (int i = 0; i < reps; ++i) {
         StepScalars sc{i, p, dt, damping, h->rho_hh, h->force_limit, 0, 0};
+        const int mode = fuse_lce ? DIAL_LCE : DIAL_ARRAYS;
         MS_CUDA(h, cudaEventRecord(ev[3 * i], st));
-        MS_CUDA(h, launch_tri_fused(h->m, h->s, sc, fuse_lce ? DIAL_LCE : DIAL_ARRAYS, h->precision, st));
+        if (cluster) MS_CUDA(h, launch_cluster_step(h->m, h->plan, h->s, sc, mode, h->precision, st));
+        else MS_CUDA(h, launch_tri_aos(h->m, h->plan, h->s, sc, mode, h->precision, st));
         MS_CUDA(h, cudaEventRecord(ev[3 * i + 1], st));
-        MS_CUDA(h, launch_node_update(h->m, h->s, sc, h->precision, st));
+        if (cluster) MS_CUDA(h, launch_halo_update(h->m, h->plan, h->s, sc, h->precision, st));
+        else MS_CUDA(h, launch_node_update(h->m, h->s, sc, h->precision, st));
         MS_CUDA(h, cudaEventRecord(ev[3 * i + 2], st));
         p ^= 1;
     }
@@ -727,6 +904,17 @@ ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial, dou
     h->cur = p;
     *ms_tri = a / reps;
     *ms_node = b / reps;
+    return MS_OK;
+}
+
+ms_status ms_plan_info(ms_handle* h, int* cluster_size, int* tris_per_cta, int* clusters, int* halo_nodes,
+                       int* path) {
+    if (!h) return MS_ERR_INVALID_ARGUMENT;
+    if (cluster_size) *cluster_size = h->have_plan ? h->plan.cs : 0;
+    if (tris_per_cta) *tris_per_cta = h->have_plan ? h->plan.tpc : 0;
+    if (clusters) *clusters = h->have_plan ? h->plan.nclusters : 0;
+    if (halo_nodes) *halo_nodes = h->have_plan ? h->plan.n_halo : -1;
+    if (path) *path = h->have_plan ? h->step_path : 1;
     return MS_OK;
 }
 

@@ -81,6 +81,70 @@ struct DevMesh {
     float* contrib_f;
 };
 
+// Cluster-tiled step (cluster.cu).  The triangles, in their Morton order, are
+// cut into tiles of cs * tpc consecutive triangles, one tile per thread-block
+// cluster of cs CTAs, tpc triangles per CTA.  A node whose every patch
+// incidence lies in one tile is "owned" by that tile: its force is summed from
+// the cluster's shared memory and it is updated by the same kernel.  Every
+// other node is a "halo" node: the contributions it receives are written to
+// HBM and a second kernel sums them.  Both sums run in ascending triangle
+// order, the order of the two-kernel path.
+struct ClusterPlan {
+    int cs;                    // CTAs per cluster (1..8)
+    int tpc;                   // triangles per CTA (<= 1024)
+    int nclusters;
+    int threads;               // threads per CTA
+    const int4* tri_idx;       // [T][2] int4: 6 patch ids, halo-slot mask, unused
+    const double* coef_aos;    // [T][24] derivative weights, per triangle contiguous
+    const float* coef_aos_f;   // [T][24] float copy (mixed precision)
+    const double4* tri_aux;    // [T]: area, cos^2, sin^2, cos*sin of the director angle
+    const double2* lce_ln;     // [T]: lambda_final, nu_ot (only when not uniform)
+    int lce_uniform;           // lambda_final and nu_ot equal on every triangle
+    const int* own_base;       // [nclusters + 1] range of each tile's owned nodes in own_nodes
+    const int* own_nodes;      // owned node ids, grouped by tile, ascending within a tile
+    const int* own_off;        // [n_owned + 1] offsets into own_ent
+    const unsigned short* own_ent;  // (rank << 13) | (index in CTA << 3) | slot, ascending triangle
+    const int* halo_nodes;     // nodes summed by the halo kernel
+    int n_halo;
+};
+
+// ---- batched ensembles (batch.cu) ----------------------------------------------
+// Many meshes stepped together: their tables are concatenated into one union
+// mesh (nodes and triangles of instance i contiguous), every triangle and
+// node carries its instance id, and each instance keeps its own parameters
+// and its own copy of the main loop's state machine (main.cpp:269-508), run
+// on the device so that long stretches need no host round trip.
+struct InstParams {
+    double timestep, damping1, damping2, rho_hh, force_limit, nu, gamma;
+    double char_force, char_speed, force_thresh, speed_thresh;
+    double spacing, lam_final, nu_ot;
+    long long steps_per_phase, steps_between_checks;
+    int node_begin, node_end;
+};
+
+enum InstStatus { INST_DIALLING = 0, INST_WAITING = 1, INST_EQUIL = 2, INST_DONE = 3, INST_FAILED = 4 };
+
+struct InstState {
+    int status;
+    int check_now;             // this step carries an equilibrium check
+    int equilibria;
+    int pad;
+    long long k_phase, since_check, stepcount;
+    double dial_factor, last_equil_dial, time, damping;
+    double cur_dial, cur_lam, cur_pw;  // dial values of the last dialled step
+    double max_force, max_speed;       // last check
+    long long max_force_node, max_speed_node;
+};
+
+struct BatchView {
+    int n_inst;
+    const int* node_inst;      // [N]
+    const InstParams* ip;      // [n_inst]
+    InstState* is;             // [n_inst]
+    double* fnorm;             // [N] |F| on check steps
+    double* vnorm;             // [N] |v| on check steps
+};
+
 struct DevState {
     double* pos[2];
     double* vel[2];
@@ -136,6 +200,28 @@ cudaError_t launch_angle_deficits(const DevMesh& m, const DevState& s, int parit
 cudaError_t launch_kinetic(const DevMesh& m, const DevState& s, int parity, double* ke /*[N]*/, cudaStream_t st);
 // Advances DevError::base by `len` after a graph chunk of `len` steps.
 cudaError_t launch_chunk_end(const DevState& s, int len, cudaStream_t st);
+
+// ---- cluster-tiled step (cluster.cu) ------------------------------------------
+// dial_mode: DIAL_ARRAYS reads abar/bbar; DIAL_LCE evaluates protocol 3 from
+// the per-step triple s.dials[3 * step] = {dial, lambda, lambda^(-2 nu)}.
+cudaError_t launch_cluster_step(const DevMesh& m, const ClusterPlan& p, const DevState& s, const StepScalars& sc,
+                                int dial_mode, int mixed, cudaStream_t st);
+cudaError_t launch_halo_update(const DevMesh& m, const ClusterPlan& p, const DevState& s, const StepScalars& sc,
+                               int mixed, cudaStream_t st);
+// Two-kernel path, per-triangle kernel over the per-triangle (AoS) tables;
+// with mixed, contributions go to DevMesh::contrib_f as float.
+cudaError_t launch_tri_aos(const DevMesh& m, const ClusterPlan& p, const DevState& s, const StepScalars& sc,
+                           int dial_mode, int mixed, cudaStream_t st);
+// Largest cluster size (8, 4, 2, 1) whose clusters fill the most SMs, and the
+// CTA shape used with it.
+int choose_cluster_size(int tpc, int threads, int mixed);
+// Shared-memory bytes per CTA of the cluster kernel.
+size_t cluster_smem_bytes(int tpc, int mixed);
+// Threads per CTA of the cluster kernel.
+int cluster_threads();
+// Raise the dynamic shared-memory limit of the cluster kernels (once, outside
+// any stream capture).
+cudaError_t prepare_cluster_kernels(int tpc);
 // Deterministic compensated sum of n doubles into *out (two passes, fixed order).
 cudaError_t launch_comp_sum(const double* x, int n, double* partial /*>= 1024*/, double* out, cudaStream_t st);
 

@@ -19,8 +19,10 @@
 #include <cfloat>
 #include <climits>
 #include <cstdint>
+#include <type_traits>
 
 #include "internal.cuh"
+#include "step_common.cuh"
 #include "tri_physics.cuh"
 
 namespace msb {
@@ -29,26 +31,12 @@ using dev::Cq;
 using dev::CqGrad;
 using dev::TriMat;
 using dev::V3;
+using namespace stepdev;
 
 namespace {
 
 constexpr int kTriBlock = 128;
 constexpr int kNodeBlock = 256;
-
-// True when an earlier step of this launch tripped the force guard; such a
-// step's input state must survive, so later kernels do nothing.
-// Buffer selection without indexing the by-value parameter arrays (a dynamic
-// index would spill the whole struct to local memory).
-__device__ __forceinline__ double* pos_buf(const DevState& s, int p) { return p ? s.pos[1] : s.pos[0]; }
-__device__ __forceinline__ double* vel_buf(const DevState& s, int p) { return p ? s.vel[1] : s.vel[0]; }
-
-__device__ __forceinline__ int global_step(const DevError* e, int local) {
-    return *((volatile const int*)&e->base) + local;
-}
-__device__ __forceinline__ bool stale(const DevError* e, int gstep) {
-    const unsigned long long key = *((volatile const unsigned long long*)&e->guard_key);
-    return key < ((unsigned long long)(unsigned)gstep << 32);
-}
 
 template <typename R>
 __device__ __forceinline__ void load_cq_from_patch(const DevMesh& m, const double* __restrict__ pos, int t,
@@ -151,7 +139,7 @@ __global__ void __launch_bounds__(kTriBlock) k_tri_fused(const DevMesh m, const 
         TriMat<double> mt;
         load_material(m, t, mt);
         if (DIAL == DIAL_LCE) {
-            const double dial = s.dials[gstep];
+            const double dial = s.dials[3 * gstep];
             dev::lce_abar(dial, __ldg(m.info_a + t), __ldg(m.info_a + (size_t)m.T + t),
                           __ldg(m.info_a + 2 * (size_t)m.T + t), mt.abar0, mt.abar1, mt.abar2);
             mt.bbar0 = mt.bbar1 = mt.bbar2 = 0.0;
@@ -193,71 +181,10 @@ __global__ void __launch_bounds__(kTriBlock) k_tri_fused(const DevMesh m, const 
 
 // Block-wide max with first-index tie-break, then the last block to finish
 // folds the per-block partials in block order.
-__device__ __forceinline__ void eq_merge(double& f, int& fn, double of, int ofn) {
-    // Larger value wins; on equal values the smaller node id wins
-    // (std::max_element returns the first maximum).  NaN never wins a
-    // comparison, as in std::max_element.
-    if (of > f || (of == f && ofn < fn)) {
-        f = of;
-        fn = ofn;
-    }
-}
-
-__device__ void eq_block_reduce_and_finish(const DevState& s, double fmax, int fnode, double vmax, int vnode) {
-    __shared__ double sf[kNodeBlock / 32], sv[kNodeBlock / 32];
-    __shared__ int sfn[kNodeBlock / 32], svn[kNodeBlock / 32];
-    __shared__ bool last;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        double of = __shfl_down_sync(0xffffffffu, fmax, o);
-        int ofn = __shfl_down_sync(0xffffffffu, fnode, o);
-        double ov = __shfl_down_sync(0xffffffffu, vmax, o);
-        int ovn = __shfl_down_sync(0xffffffffu, vnode, o);
-        eq_merge(fmax, fnode, of, ofn);
-        eq_merge(vmax, vnode, ov, ovn);
-    }
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) {
-        sf[warp] = fmax;
-        sfn[warp] = fnode;
-        sv[warp] = vmax;
-        svn[warp] = vnode;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double F = sf[0], V = sv[0];
-        int Fn = sfn[0], Vn = svn[0];
-        for (int w = 1; w < kNodeBlock / 32; ++w) {
-            eq_merge(F, Fn, sf[w], sfn[w]);
-            eq_merge(V, Vn, sv[w], svn[w]);
-        }
-        s.eq_part[blockIdx.x] = {F, V, Fn, Vn};
-        __threadfence();
-        unsigned int done = atomicAdd(s.eq_counter, 1u);
-        last = (done == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-        __threadfence();
-        double F = -1.0, V = -1.0;
-        int Fn = INT_MAX, Vn = INT_MAX;
-        for (unsigned int b = 0; b < gridDim.x; ++b) {
-            const volatile EqPartial* p = s.eq_part + b;
-            eq_merge(F, Fn, p->f, p->fn);
-            eq_merge(V, Vn, p->v, p->vn);
-        }
-        s.equil->max_force = F;
-        s.equil->max_speed = V;
-        s.equil->max_force_node = Fn;
-        s.equil->max_speed_node = Vn;
-        *s.eq_counter = 0u;
-    }
-}
-
-__device__ __forceinline__ void record_guard(const DevState& s, int step, long long dof) {
-    unsigned long long key = ((unsigned long long)(unsigned)step << 32) | (unsigned long long)dof;
-    atomicMin(&s.err->guard_key, key);
-    atomicExch(&s.err->flag, 3);  // MS_ERR_IMPLAUSIBLE_FORCE
+__device__ __forceinline__ void eq_block_reduce_and_finish(const DevState& s, double fmax, int fnode, double vmax,
+                                                           int vnode) {
+    const EqPartial r = eq_block_reduce<kNodeBlock>(fmax, fnode, vmax, vnode);
+    eq_store_and_fold(s, r, blockIdx.x, gridDim.x, gridDim.x);
 }
 
 template <bool MIXED>
@@ -271,67 +198,38 @@ __global__ void __launch_bounds__(kNodeBlock) k_node_update(const DevMesh m, con
     if (n < N) {
         const int b = __ldg(m.inc_off + n), e = __ldg(m.inc_off + n + 1);
         double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-        const double* __restrict__ c = s.contrib;
+        using Cf = typename std::conditional<MIXED, float, double>::type;
+        const Cf* __restrict__ c;
+        if constexpr (MIXED) c = m.contrib_f;
+        else c = s.contrib;
+        // Indices eight at a time, then all their contributions, so that a
+        // node's loads are in flight together; the sum stays in entry order.
         int k = b;
-        for (; k + 3 < e; k += 4) {
-            const int e0 = __ldg(m.inc_ent + k), e1 = __ldg(m.inc_ent + k + 1), e2 = __ldg(m.inc_ent + k + 2),
-                      e3 = __ldg(m.inc_ent + k + 3);
-            const double a0 = c[3 * (size_t)e0], a1 = c[3 * (size_t)e0 + 1], a2 = c[3 * (size_t)e0 + 2];
-            const double b0 = c[3 * (size_t)e1], b1 = c[3 * (size_t)e1 + 1], b2 = c[3 * (size_t)e1 + 2];
-            const double c0 = c[3 * (size_t)e2], c1 = c[3 * (size_t)e2 + 1], c2 = c[3 * (size_t)e2 + 2];
-            const double d0 = c[3 * (size_t)e3], d1 = c[3 * (size_t)e3 + 1], d2 = c[3 * (size_t)e3 + 2];
-            Fx += a0; Fy += a1; Fz += a2;
-            Fx += b0; Fy += b1; Fz += b2;
-            Fx += c0; Fy += c1; Fz += c2;
-            Fx += d0; Fy += d1; Fz += d2;
+        for (; k + 7 < e; k += 8) {
+            int ei[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) ei[j] = __ldg(m.inc_ent + k + j);
+            Cf v[8][3];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                v[j][0] = c[3 * (size_t)ei[j]];
+                v[j][1] = c[3 * (size_t)ei[j] + 1];
+                v[j][2] = c[3 * (size_t)ei[j] + 2];
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                Fx += (double)v[j][0];
+                Fy += (double)v[j][1];
+                Fz += (double)v[j][2];
+            }
         }
         for (; k < e; ++k) {
             const int e0 = __ldg(m.inc_ent + k);
-            Fx += c[3 * (size_t)e0];
-            Fy += c[3 * (size_t)e0 + 1];
-            Fz += c[3 * (size_t)e0 + 2];
+            Fx += (double)c[3 * (size_t)e0];
+            Fy += (double)c[3 * (size_t)e0 + 1];
+            Fz += (double)c[3 * (size_t)e0 + 2];
         }
-        const double* pos = pos_buf(s, sc.parity);
-        const double* vel = vel_buf(s, sc.parity);
-        const double vx = vel[n], vy = vel[N + n], vz = vel[2 * N + n];
-        const double mass = __ldg(m.mass + n);
-        if (!sc.gd) {
-            const double dm = -sc.damping * mass;
-            Fx += dm * vx / sc.rho_hh;
-            Fy += dm * vy / sc.rho_hh;
-            Fz += dm * vz / sc.rho_hh;
-        }
-        if (__ldg(m.fixed + n)) Fx = Fy = Fz = 0.0;
-        if (sc.check) {
-            fmax = sqrt(Fx * Fx + Fy * Fy + Fz * Fz);
-            vmax = sqrt(vx * vx + vy * vy + vz * vz);
-            fnode = n;
-            vnode = n;
-        }
-        const double lim = sc.force_limit;
-        if (!(fabs(Fx) < lim)) record_guard(s, gstep, (long long)n);
-        if (!(fabs(Fy) < lim)) record_guard(s, gstep, (long long)N + n);
-        if (!(fabs(Fz) < lim)) record_guard(s, gstep, 2LL * N + n);
-        double nvx, nvy, nvz;
-        if (!sc.gd) {
-            const double k2 = sc.dt / mass;
-            nvx = vx + k2 * Fx;
-            nvy = vy + k2 * Fy;
-            nvz = vz + k2 * Fz;
-        } else {
-            const double den = sc.damping * mass;
-            nvx = sc.rho_hh * Fx / den;
-            nvy = sc.rho_hh * Fy / den;
-            nvz = sc.rho_hh * Fz / den;
-        }
-        double* npos = pos_buf(s, sc.parity ^ 1);
-        double* nvel = vel_buf(s, sc.parity ^ 1);
-        npos[n] = pos[n] + sc.dt * nvx;
-        npos[N + n] = pos[N + n] + sc.dt * nvy;
-        npos[2 * N + n] = pos[2 * N + n] + sc.dt * nvz;
-        nvel[n] = nvx;
-        nvel[N + n] = nvy;
-        nvel[2 * N + n] = nvz;
+        node_finish(m, s, sc, gstep, n, Fx, Fy, Fz, fmax, fnode, vmax, vnode);
     }
     if (sc.check) eq_block_reduce_and_finish(s, fmax, fnode, vmax, vnode);
 }
@@ -784,7 +682,8 @@ cudaError_t launch_node_update(const DevMesh& m, const DevState& s, const StepSc
                                cudaStream_t st) {
     const int nb = blocks_for(m.N, kNodeBlock);
     (void)mixed;
-    k_node_update<false><<<nb, kNodeBlock, 0, st>>>(m, s, sc);
+    if (mixed) k_node_update<true><<<nb, kNodeBlock, 0, st>>>(m, s, sc);
+    else k_node_update<false><<<nb, kNodeBlock, 0, st>>>(m, s, sc);
     return cudaGetLastError();
 }
 

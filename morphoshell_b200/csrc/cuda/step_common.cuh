@@ -1,0 +1,158 @@
+// Device helpers shared by the two fused-step implementations (kernels.cu:
+// triangle kernel + node kernel; cluster.cu: cluster-tiled kernel + halo
+// kernel), so both apply exactly the same per-node arithmetic.
+#pragma once
+
+#include <climits>
+
+#include "internal.cuh"
+
+namespace msb {
+namespace stepdev {
+
+// Buffer selection without indexing the by-value parameter arrays (a dynamic
+// index would spill the whole struct to local memory).
+__device__ __forceinline__ double* pos_buf(const DevState& s, int p) { return p ? s.pos[1] : s.pos[0]; }
+__device__ __forceinline__ double* vel_buf(const DevState& s, int p) { return p ? s.vel[1] : s.vel[0]; }
+
+__device__ __forceinline__ int global_step(const DevError* e, int local) {
+    return *((volatile const int*)&e->base) + local;
+}
+// True when an earlier step of this launch tripped the force guard; such a
+// step's input state must survive, so later kernels do nothing.
+__device__ __forceinline__ bool stale(const DevError* e, int gstep) {
+    const unsigned long long key = *((volatile const unsigned long long*)&e->guard_key);
+    return key < ((unsigned long long)(unsigned)gstep << 32);
+}
+
+__device__ __forceinline__ void record_guard(const DevState& s, int gstep, long long dof) {
+    const unsigned long long key = ((unsigned long long)(unsigned)gstep << 32) | (unsigned long long)dof;
+    atomicMin(&s.err->guard_key, key);
+    atomicExch(&s.err->flag, 3);  // MS_ERR_IMPLAUSIBLE_FORCE
+}
+
+// Larger value wins; on equal values the smaller node id wins
+// (std::max_element returns the first maximum).  NaN never wins a
+// comparison, as in std::max_element.
+__device__ __forceinline__ void eq_merge(double& f, int& fn, double of, int ofn) {
+    if (of > f || (of == f && ofn < fn)) {
+        f = of;
+        fn = ofn;
+    }
+}
+
+// Block-wide max/argmax of |F| and |v|; the result is valid in thread 0.
+// BLOCK is the block size (a multiple of 32, at most 1024).
+template <int BLOCK>
+__device__ __forceinline__ EqPartial eq_block_reduce(double fmax, int fnode, double vmax, int vnode) {
+    __shared__ double sf[BLOCK / 32], sv[BLOCK / 32];
+    __shared__ int sfn[BLOCK / 32], svn[BLOCK / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double of = __shfl_down_sync(0xffffffffu, fmax, o);
+        const int ofn = __shfl_down_sync(0xffffffffu, fnode, o);
+        const double ov = __shfl_down_sync(0xffffffffu, vmax, o);
+        const int ovn = __shfl_down_sync(0xffffffffu, vnode, o);
+        eq_merge(fmax, fnode, of, ofn);
+        eq_merge(vmax, vnode, ov, ovn);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        sf[warp] = fmax;
+        sfn[warp] = fnode;
+        sv[warp] = vmax;
+        svn[warp] = vnode;
+    }
+    __syncthreads();
+    EqPartial r{-1.0, -1.0, INT_MAX, INT_MAX};
+    if (threadIdx.x == 0) {
+        r = {sf[0], sv[0], sfn[0], svn[0]};
+        for (int w = 1; w < BLOCK / 32; ++w) {
+            eq_merge(r.f, r.fn, sf[w], sfn[w]);
+            eq_merge(r.v, r.vn, sv[w], svn[w]);
+        }
+    }
+    return r;
+}
+
+// Thread 0 of each block stores its partial at eq_part[slot] and counts; the
+// last of `counted` blocks folds eq_part[0 .. total) in index order.
+__device__ __forceinline__ void eq_store_and_fold(const DevState& s, const EqPartial& r, int slot, unsigned counted,
+                                                  int total) {
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        s.eq_part[slot] = r;
+        __threadfence();
+        const unsigned done = atomicAdd(s.eq_counter, 1u);
+        last = (done == counted - 1);
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        double F = -1.0, V = -1.0;
+        int Fn = INT_MAX, Vn = INT_MAX;
+        for (int b = 0; b < total; ++b) {
+            const volatile EqPartial* p = s.eq_part + b;
+            eq_merge(F, Fn, p->f, p->fn);
+            eq_merge(V, Vn, p->v, p->vn);
+        }
+        s.equil->max_force = F;
+        s.equil->max_speed = V;
+        s.equil->max_force_node = Fn;
+        s.equil->max_speed_node = Vn;
+        *s.eq_counter = 0u;
+    }
+}
+
+// Everything after the deformation-force sum for one node: damping
+// (calc_non_deformation_forces.cpp:44-57), constraints (impose_constraints.cpp:56-68),
+// the equilibrium maxima (is_at_equilibrium.cpp:62-76), the force guard and
+// the symplectic-Euler update (advance_dynamics.cpp:58-93) into the other
+// ping-pong buffer.
+__device__ __forceinline__ void node_finish(const DevMesh& m, const DevState& s, const StepScalars& sc, int gstep,
+                                            int n, double Fx, double Fy, double Fz, double& fmax, int& fnode,
+                                            double& vmax, int& vnode) {
+    const int N = m.N;
+    const double* pos = pos_buf(s, sc.parity);
+    const double* vel = vel_buf(s, sc.parity);
+    const double vx = vel[n], vy = vel[N + n], vz = vel[2 * N + n];
+    const double mass = __ldg(m.mass + n);
+    if (!sc.gd) {
+        const double dm = -sc.damping * mass;
+        Fx += dm * vx / sc.rho_hh;
+        Fy += dm * vy / sc.rho_hh;
+        Fz += dm * vz / sc.rho_hh;
+    }
+    if (__ldg(m.fixed + n)) Fx = Fy = Fz = 0.0;
+    if (sc.check) {
+        eq_merge(fmax, fnode, sqrt(Fx * Fx + Fy * Fy + Fz * Fz), n);
+        eq_merge(vmax, vnode, sqrt(vx * vx + vy * vy + vz * vz), n);
+    }
+    const double lim = sc.force_limit;
+    if (!(fabs(Fx) < lim)) record_guard(s, gstep, (long long)n);
+    if (!(fabs(Fy) < lim)) record_guard(s, gstep, (long long)N + n);
+    if (!(fabs(Fz) < lim)) record_guard(s, gstep, 2LL * N + n);
+    double nvx, nvy, nvz;
+    if (!sc.gd) {
+        const double k2 = sc.dt / mass;
+        nvx = vx + k2 * Fx;
+        nvy = vy + k2 * Fy;
+        nvz = vz + k2 * Fz;
+    } else {
+        const double den = sc.damping * mass;
+        nvx = sc.rho_hh * Fx / den;
+        nvy = sc.rho_hh * Fy / den;
+        nvz = sc.rho_hh * Fz / den;
+    }
+    double* npos = pos_buf(s, sc.parity ^ 1);
+    double* nvel = vel_buf(s, sc.parity ^ 1);
+    npos[n] = pos[n] + sc.dt * nvx;
+    npos[N + n] = pos[N + n] + sc.dt * nvy;
+    npos[2 * N + n] = pos[2 * N + n] + sc.dt * nvz;
+    nvel[n] = nvx;
+    nvel[N + n] = nvy;
+    nvel[2 * N + n] = nvz;
+}
+
+}  // namespace stepdev
+}  // namespace msb

@@ -93,18 +93,37 @@ __device__ __forceinline__ R quad_form(R abar0, R abar1, R abar2, R d0, R d1, R 
     return w;
 }
 
+// Stretch and bend prefactors sp, bp of one triangle (they hold the metric
+// inverse through det(abar)^(-3/2)).
+template <typename R>
+__device__ __forceinline__ void prefactors(const TriMat<R>& m, R nu, R& sp, R& bp) {
+    const R det = m.abar0 * m.abar2 - m.abar1 * m.abar1;
+    const R inv_det = R(1) / det;
+    const R det_m32 = inv_det * rsqrt_r(det);
+    const R omn = R(1) - nu;
+    sp = R(2) * m.h * m.mu * det_m32 / omn;
+    bp = m.mu * m.h * m.h * m.h * det_m32 / (R(6) * omn);
+}
+
+template <typename R>
+__device__ __forceinline__ void energy_gradient_pref(const Cq<R>& c, const TriMat<R>& m, R nu, R gamma, R sp, R bp,
+                                                     CqGrad<R>& g, R* w_stretch = nullptr, R* w_bend = nullptr);
+
 // Energy gradient of one triangle.  Also returns the stretch and bend
 // (stiffened) energy densities, used by the energy reductions.
 template <typename R>
 __device__ __forceinline__ void energy_gradient(const Cq<R>& c, const TriMat<R>& m, R nu, R gamma, CqGrad<R>& g,
                                                 R* w_stretch = nullptr, R* w_bend = nullptr) {
-    const R det = m.abar0 * m.abar2 - m.abar1 * m.abar1;
-    const R inv_det = R(1) / det;
-    const R det_m32 = inv_det * rsqrt_r(det);
-    const R omn = R(1) - nu;
-    const R sp = R(2) * m.h * m.mu * det_m32 / omn;
-    const R bp = m.mu * m.h * m.h * m.h * det_m32 / (R(6) * omn);
+    R sp, bp;
+    prefactors(m, nu, sp, bp);
+    energy_gradient_pref(c, m, nu, gamma, sp, bp, g, w_stretch, w_bend);
+}
 
+// The same with the prefactors given (the mixed-precision path forms them in
+// double and passes them rounded to float).
+template <typename R>
+__device__ __forceinline__ void energy_gradient_pref(const Cq<R>& c, const TriMat<R>& m, R nu, R gamma, R sp, R bp,
+                                                     CqGrad<R>& g, R* w_stretch, R* w_bend) {
     // Stretch.
     const R a0 = dot(c.rx, c.rx), a1 = dot(c.rx, c.ry), a2 = dot(c.ry, c.ry);
     R qs0, qs1, qs2;

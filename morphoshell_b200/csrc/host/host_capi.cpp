@@ -506,6 +506,7 @@ int msh_run(msh_model* model, const msh_run_options* opts, msh_run_result* res, 
             // equilibrium reached at full dial factor instead.
             if (st.status == equil_reached && last_equil_dial >= 1.0 && opts->stop_at_final_equilibrium) {
                 res->final_status = st.status;
+                dial_factor = last_equil_dial;  // report the dial factor equilibrium was reached at
                 break;
             }
             if (st.status == equil_reached) {  // :501-507
