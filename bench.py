@@ -46,8 +46,10 @@ sys.path.insert(0, ROOT)
 # (24 B), 24 derivative weights (192 B), 3 abar_info columns (24 B) and the
 # reference area (8 B); per node read+write of position and velocity
 # (96 B) and the mass (8 B), i.e. 104 B per node = 52 B per triangle at
-# N = T/2.  Mixed precision reads the 24 weights and the area as float.
-BYTES_PER_TRI = {"fp64": 24 + 192 + 24 + 8 + 52, "mixed": 24 + 96 + 24 + 4 + 52}
+# N = T/2.  Mixed precision reads the 24 weights as float (the director
+# trigonometry and the area stay double: they set abar, which the strain
+# a - abar is formed against in double).
+BYTES_PER_TRI = {"fp64": 24 + 192 + 24 + 8 + 52, "mixed": 24 + 96 + 24 + 8 + 52}
 METRIC = "tri-steps/s"
 
 
@@ -321,10 +323,10 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": ("one step = k_cluster_step + k_halo_update" if args.path == "cluster"
-                                else "one step = k_tri_fused + k_node_update"),
+                                else "one step = k_tri_aos + k_node_update"),
                      "algorithmic_bytes_per_tri": bpt,
                      "kernel_ms": ({"k_cluster_step": t_tri, "k_halo_update": t_node} if args.path == "cluster"
-                                   else {"k_tri_fused": t_tri, "k_node_update": t_node})},
+                                   else {"k_tri_aos": t_tri, "k_node_update": t_node})},
         "plan": plan,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 2 * 24 * N + 8,
                 "d2h_bytes_per_step": 2 * 24 * N + 16, "steps": e2e_steps},
@@ -333,6 +335,91 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(model, info, bbar)
     g.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ensemble(args):
+    """``--workload ensembleN`` (default N = 256): N independent disks in one
+    batch (ms_batch_*), spacing log-uniform in [0.004, 0.02], lambda_final
+    ~ U(0.8, 1.2), defect charge from {+1, -1, +1/2} (director angle =
+    charge * theta), thickness ~ U(0.005, 0.02), seed 7.  Every instance
+    runs its own dialling / equilibrium state machine on the device; the
+    timed steps are ms_batch_run over the whole ensemble.  One GPU holds
+    the whole ensemble; with N GPUs each rank runs its own ensemble."""
+    import torch
+    from morphoshell_b200 import MS_PRECISION_FP64, MS_PRECISION_MIXED, Batch, ensemble
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800),
+                                device_id=torch.device("cuda", local))
+    n = int(args.workload[len("ensemble"):] or 256)
+    t0 = time.time()
+    cores = os.cpu_count() or 8
+    models, params = ensemble.build_members(range(n), tempfile.mkdtemp(prefix="ms_ens_"), seed=7,
+                                            threads=cores, processes=min(cores, 32))
+    setup_s = time.time() - t0
+    log("ensemble of %d built in %.1f s" % (n, setup_s))
+    prec = MS_PRECISION_MIXED if args.precision == "mixed" else MS_PRECISION_FP64
+    b = Batch(models, precision=prec, device=local)
+    info = b.info()
+    T = info["num_tris"]
+    sched, tune_ms = b.autotune(steps_per_trial=8)
+    b.run(args.warmup)
+    stream = torch.cuda.ExternalStream(b.stream(), device=torch.device("cuda", local))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        done = b.run(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = T * done * world / (ms_max / 1e3)
+    bpt = BYTES_PER_TRI[args.precision]
+    achieved = bpt * T / (ms_max / done / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    sizes = [p["num_tris"] for p in params]
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": done, "warmup": args.warmup,
+        "ms_per_step": ms_max / done, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed", "data": "synthetic",
+        "config": {"workload": "ensemble%d: %d unit disks in one batch, spacing log-uniform [0.004, 0.02] "
+                               "(%d..%d triangles, %d in all), lambda_final ~ U(0.8, 1.2), charge in "
+                               "{+1, -1, +1/2}, h ~ U(0.005, 0.02), per-instance dialling state machines"
+                               % (n, n, min(sizes), max(sizes), T),
+                   "precision": args.precision, "num_tris": T, "num_nodes": info["num_nodes"],
+                   "instances": n, "schedule": sched, "autotune_ms_per_step": tune_ms,
+                   "host_setup_s": setup_s, "parallelism": "replicas x%d" % world,
+                   "l2": "inputs far larger than L2; no flush"},
+        "gpu_launches": 4 * done,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "kernel": "one step = k_batch_pre + k_batch_tri + k_batch_node + k_batch_post (whole step)",
+                     "algorithmic_bytes_per_tri": bpt},
+        "clocks": clk.summary(),
+    }
+    b.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -350,12 +437,14 @@ def main():
     ap.add_argument("--workload", default="disk1p8m")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
-    ap.add_argument("--path", choices=["cluster", "two-kernel"], default="cluster",
+    ap.add_argument("--path", choices=["cluster", "two-kernel"], default="two-kernel",
                     help="fused-step implementation (ms_set_step_path)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload.startswith("ensemble"):
+        return run_ensemble(args)
     return run_ours(args)
 
 

@@ -200,12 +200,13 @@ ms_status ms_device_info(char* buf, size_t len);
  * or time their own work around it. */
 void* ms_stream(ms_handle* h);
 
-/* Which implementation ms_step_n uses: 0 (default) the cluster-tiled step --
- * each thread-block cluster owns a Morton tile of triangles, keeps their
- * force contributions in distributed shared memory and updates the tile's
- * interior nodes itself; 1 the two-kernel step (per-triangle kernel writes
- * all contributions to HBM, per-node kernel gathers them).  Both sum every
- * node's contributions in ascending triangle order. */
+/* Which implementation ms_step_n uses: 0 the cluster-tiled step -- each
+ * thread-block cluster owns a Morton tile of triangles, keeps their force
+ * contributions in distributed shared memory and updates the tile's
+ * interior nodes itself; 1 (default) the two-kernel step (per-triangle
+ * kernel writes all contributions to HBM, per-node kernel gathers them).
+ * Both sum every node's contributions in ascending triangle order, so they
+ * give the same bits. */
 ms_status ms_set_step_path(ms_handle* h, int path);
 /* Tiling of the cluster path: CTAs per cluster, triangles per CTA, number of
  * clusters, number of halo nodes (summed by the second kernel), and the
@@ -218,6 +219,88 @@ ms_status ms_plan_info(ms_handle* h, int* cluster_size, int* tris_per_cta, int* 
  * the per-triangle kernel (ms_tri) and the per-node kernel (ms_node). */
 ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial_factor, double timestep,
                           double damping_factor, double* ms_tri, double* ms_node);
+
+/* ---- batched ensembles -----------------------------------------------------
+ * Many independent meshes of any sizes stepped together on one device.  No
+ * reference counterpart: the reference runs one mesh per process, and each
+ * instance here runs its own copy of that process's main loop
+ * (main.cpp:269-508) on the device -- protocol-3 dialling, the wait for
+ * equilibrium with checks every timesteps_between_equil_checks steps
+ * (is_at_equilibrium.cpp:51-99), the next dial phase, the force guard
+ * (advance_dynamics.cpp:58-75) -- with its own timestep, damping,
+ * thresholds and programmed field.  An instance that trips the guard is
+ * marked failed and keeps the state from before that step; one that reaches
+ * equilibrium at dial factor 1 (with stop_at_final_equilibrium) is done;
+ * either way it stops while the others go on.  Steps run in chunks captured
+ * as CUDA graphs; the host looks at the instance states between chunks. */
+typedef struct ms_batch ms_batch;
+
+enum ms_inst_status {
+    MS_INST_DIALLING = 0,
+    MS_INST_WAITING = 1,   /* waiting_for_equil */
+    MS_INST_EQUIL = 2,     /* transient: equilibrium reached this step */
+    MS_INST_DONE = 3,      /* equilibrium reached at dial factor 1 */
+    MS_INST_FAILED = 4     /* force guard tripped */
+};
+
+typedef struct ms_batch_instance {
+    ms_mesh_desc mesh;
+    ms_params params;
+    /* Protocol-3 programmed field, T x 3 row-major (director angle,
+     * lambda_final, nu_ot), as abar_info of do_dialling.cpp:112-123;
+     * lambda_final and nu_ot must be the same on every triangle. */
+    const double* abar_info;
+    double timestep;
+    double damping_factor_1, damping_factor_2;  /* dialling, waiting */
+    int64_t timesteps_per_dial_phase;
+    int64_t timesteps_between_equil_checks;
+    double dial_factors_to_hold_at_spacing;
+    double dial_factor_to_start_from;
+    int32_t stop_at_final_equilibrium;
+    const double* dofs;        /* 3N initial positions, SoA */
+    const double* velocities;  /* 3N or NULL (zero) */
+} ms_batch_instance;
+
+typedef struct ms_batch_inst_status {
+    int32_t status;            /* ms_inst_status */
+    int32_t equilibria;        /* equilibria reached so far */
+    int64_t stepcount;
+    double dial_factor, last_equil_dial, sim_time;
+    double max_force_ratio, max_speed_ratio;  /* at the last check */
+    int64_t max_force_node, max_speed_node;
+    int64_t offending_dof;     /* failed: dof (SoA, within the instance) whose force tripped the guard, else -1 */
+} ms_batch_inst_status;
+
+/* Launch schedule: threads per block of the per-triangle and per-node
+ * kernels, steps per captured graph (even). */
+typedef struct ms_batch_schedule {
+    int32_t tri_block, node_block, chunk_steps;
+} ms_batch_schedule;
+
+/* Only dialling protocol 3 without ansatz dialling and Newtonian dynamics
+ * (no gradient-descent steps) are batched. */
+ms_status ms_batch_create(const ms_batch_instance* instances, int32_t n_instances, int32_t device,
+                          int32_t precision, ms_batch** out);
+void ms_batch_destroy(ms_batch* b);
+const char* ms_batch_last_error(const ms_batch* b);
+/* Runs up to max_steps steps, or until every instance is done or failed;
+ * *steps_done receives the steps run. */
+ms_status ms_batch_run(ms_batch* b, int64_t max_steps, int64_t* steps_done);
+ms_status ms_batch_status(ms_batch* b, int32_t instance, ms_batch_inst_status* out);
+/* Current (or final) positions and velocities of one instance, SoA; either may be NULL. */
+ms_status ms_batch_download_dofs(ms_batch* b, int32_t instance, double* dofs, double* velocities);
+/* Replaces one instance's positions (and velocities; NULL = zero), e.g. a
+ * warm start, and restarts its state machine from dial_factor_to_start_from. */
+ms_status ms_batch_upload_dofs(ms_batch* b, int32_t instance, const double* dofs, const double* velocities);
+ms_status ms_batch_set_schedule(ms_batch* b, const ms_batch_schedule* s);
+ms_status ms_batch_get_schedule(const ms_batch* b, ms_batch_schedule* s);
+/* Times every built-in schedule on this batch (steps_per_trial steps each,
+ * CUDA events) from the current state, puts the state back after each trial,
+ * and keeps the fastest.  All schedules give the same bits. */
+ms_status ms_batch_autotune(ms_batch* b, int32_t steps_per_trial, ms_batch_schedule* chosen,
+                            double* best_ms_per_step);
+ms_status ms_batch_info(const ms_batch* b, int64_t* num_nodes, int64_t* num_tris, int32_t* n_instances);
+void* ms_batch_stream(ms_batch* b);
 
 #ifdef __cplusplus
 }

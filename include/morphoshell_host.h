@@ -95,6 +95,15 @@ typedef struct msh_run_result {
 /* Runs the dynamics loop; dofs_out (3N, may be NULL) receives the final state. */
 int msh_run(msh_model* m, const msh_run_options* opts, msh_run_result* res, double* dofs_out);
 
+/* Runs n models together as one batch (ms_batch_*): every model follows
+ * msh_run's loop independently; max_steps bounds the batch's steps.  No
+ * reference counterpart (the reference runs one mesh per process).  Needs
+ * protocol-3 dialling from the reference state and Newtonian dynamics;
+ * write_outputs and output_dir are ignored.  results[i] and dofs_out[i]
+ * (3N_i or NULL; dofs_out itself may be NULL) receive each model's outcome. */
+int msh_run_batch(msh_model* const* models, int32_t n, const msh_run_options* opts, msh_run_result* results,
+                  double* const* dofs_out);
+
 #ifdef __cplusplus
 }
 #endif

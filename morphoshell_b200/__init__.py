@@ -28,10 +28,13 @@ GPU_SYMBOLS = [
     "ms_non_deformation_forces", "ms_impose_constraints", "ms_is_at_equilibrium", "ms_advance_dynamics",
     "ms_step_n", "ms_output_quantities", "ms_device_info", "ms_stream", "ms_time_kernels",
     "ms_deformation_forces_noalloc", "ms_set_step_path", "ms_plan_info",
+    "ms_batch_create", "ms_batch_destroy", "ms_batch_last_error", "ms_batch_run", "ms_batch_status",
+    "ms_batch_download_dofs", "ms_batch_upload_dofs", "ms_batch_set_schedule", "ms_batch_get_schedule",
+    "ms_batch_autotune", "ms_batch_info", "ms_batch_stream",
 ]
 HOST_SYMBOLS = [
     "msh_load", "msh_build", "msh_free", "msh_last_error", "msh_get_scalars", "msh_get_desc", "msh_get_dofs",
-    "msh_get_programmed", "msh_get_tri_vertices", "msh_get_boundary", "msh_run",
+    "msh_get_programmed", "msh_get_tri_vertices", "msh_get_boundary", "msh_run", "msh_run_batch",
 ]
 
 
@@ -92,6 +95,28 @@ class msh_run_result(C.Structure):
                 ("last_max_speed_ratio", C.c_double)]
 
 
+class ms_batch_instance(C.Structure):
+    _fields_ = [("mesh", ms_mesh_desc), ("params", ms_params), ("abar_info", C.POINTER(C.c_double)),
+                ("timestep", C.c_double), ("damping_factor_1", C.c_double), ("damping_factor_2", C.c_double),
+                ("timesteps_per_dial_phase", C.c_int64), ("timesteps_between_equil_checks", C.c_int64),
+                ("dial_factors_to_hold_at_spacing", C.c_double), ("dial_factor_to_start_from", C.c_double),
+                ("stop_at_final_equilibrium", C.c_int32), ("dofs", C.POINTER(C.c_double)),
+                ("velocities", C.POINTER(C.c_double))]
+
+
+class ms_batch_inst_status(C.Structure):
+    _fields_ = [("status", C.c_int32), ("equilibria", C.c_int32), ("stepcount", C.c_int64),
+                ("dial_factor", C.c_double), ("last_equil_dial", C.c_double), ("sim_time", C.c_double),
+                ("max_force_ratio", C.c_double), ("max_speed_ratio", C.c_double), ("max_force_node", C.c_int64),
+                ("max_speed_node", C.c_int64), ("offending_dof", C.c_int64)]
+
+
+class ms_batch_schedule(C.Structure):
+    _fields_ = [("tri_block", C.c_int32), ("node_block", C.c_int32), ("chunk_steps", C.c_int32)]
+
+
+MS_INST_DIALLING, MS_INST_WAITING, MS_INST_EQUIL, MS_INST_DONE, MS_INST_FAILED = range(5)
+
 _lib = None
 
 
@@ -138,6 +163,24 @@ def lib() -> C.CDLL:
         L.ms_stream.argtypes = [C.c_void_p]
         L.ms_stream.restype = C.c_void_p
         L.ms_time_kernels.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, d, d]
+        L.ms_batch_create.argtypes = [P(ms_batch_instance), C.c_int32, C.c_int32, C.c_int32, P(C.c_void_p)]
+        L.ms_batch_destroy.argtypes = [C.c_void_p]
+        L.ms_batch_destroy.restype = None
+        L.ms_batch_last_error.argtypes = [C.c_void_p]
+        L.ms_batch_last_error.restype = C.c_char_p
+        L.ms_batch_run.argtypes = [C.c_void_p, C.c_int64, P(C.c_int64)]
+        L.ms_batch_status.argtypes = [C.c_void_p, C.c_int32, P(ms_batch_inst_status)]
+        L.ms_batch_download_dofs.argtypes = [C.c_void_p, C.c_int32, d, d]
+        L.ms_batch_upload_dofs.argtypes = [C.c_void_p, C.c_int32, d, d]
+        L.ms_batch_set_schedule.argtypes = [C.c_void_p, P(ms_batch_schedule)]
+        L.ms_batch_get_schedule.argtypes = [C.c_void_p, P(ms_batch_schedule)]
+        L.ms_batch_autotune.argtypes = [C.c_void_p, C.c_int32, P(ms_batch_schedule), d]
+        i64p = C.POINTER(C.c_int64)
+        L.ms_batch_info.argtypes = [C.c_void_p, i64p, i64p, P(C.c_int32)]
+        L.ms_batch_stream.argtypes = [C.c_void_p]
+        L.ms_batch_stream.restype = C.c_void_p
+        L.msh_run_batch.argtypes = [P(C.c_void_p), C.c_int32, P(msh_run_options), P(msh_run_result),
+                                    P(C.POINTER(C.c_double))]
         L.msh_load.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, P(C.c_void_p)]
         L.msh_build.argtypes = [C.c_char_p, C.c_int32, C.c_int32, d, P(C.c_int32), d, C.c_int32, d, C.c_int32,
                                 d, d, P(C.c_uint8), C.c_int, P(C.c_void_p)]
@@ -396,6 +439,119 @@ class GpuLoop:
                                              _dp(en)), "output_quantities")
         return {"curvatures": curv, "energy_densities": ed, "strains": strain, "stresses": stress,
                 "angle_deficits": dfc, "energies": en}
+
+
+class Batch:
+    """Many Models stepped together on one device (ms_batch_*): each runs its
+    own dialling / waiting / equilibrium state machine; see
+    include/morphoshell_gpu.h."""
+
+    def __init__(self, models, precision: int = MS_PRECISION_FP64, device: int = -1, dofs=None,
+                 stop_at_final_equilibrium: bool = True):
+        L = lib()
+        n = len(models)
+        arr = (ms_batch_instance * n)()
+        self._keep = []
+        for i, m in enumerate(models):
+            s = m.scalars
+            a_info, _ = m.programmed()
+            if a_info.shape[1] < 3:
+                raise ValueError("instance %d: protocol-3 abar_info needs 3 columns" % i)
+            info = np.ascontiguousarray(a_info[:, :3], dtype=np.float64)
+            x0 = _f64(m.dofs(1) if dofs is None or dofs[i] is None else dofs[i])
+            self._keep += [info, x0]
+            it = arr[i]
+            it.mesh = m.desc
+            it.params = m.params
+            it.abar_info = _dp(info)
+            it.timestep = s.timestep
+            it.damping_factor_1 = s.damping_factor_1
+            it.damping_factor_2 = s.damping_factor_2
+            it.timesteps_per_dial_phase = s.timesteps_per_dial_phase
+            it.timesteps_between_equil_checks = s.timesteps_between_equil_checks
+            it.dial_factors_to_hold_at_spacing = s.dial_factors_to_hold_at_spacing
+            it.dial_factor_to_start_from = s.dial_factor_to_start_from
+            it.stop_at_final_equilibrium = int(stop_at_final_equilibrium)
+            it.dofs = _dp(x0)
+            it.velocities = None
+        h = C.c_void_p()
+        rc = L.ms_batch_create(arr, n, device, precision, C.byref(h))
+        if rc != MS_OK:
+            raise MsError(rc, "ms_batch_create: %s" % L.ms_status_string(rc).decode())
+        self._h = h
+        self.models = list(models)
+        self.n = n
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ms_batch_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def _chk(self, rc, what):
+        if rc != MS_OK:
+            raise MsError(rc, "%s: %s (%s)" % (what, lib().ms_status_string(rc).decode(),
+                                                lib().ms_batch_last_error(self._h).decode()))
+
+    def run(self, max_steps: int) -> int:
+        done = C.c_int64()
+        self._chk(lib().ms_batch_run(self._h, max_steps, C.byref(done)), "ms_batch_run")
+        return done.value
+
+    def status(self, i: int) -> ms_batch_inst_status:
+        st = ms_batch_inst_status()
+        self._chk(lib().ms_batch_status(self._h, i, C.byref(st)), "ms_batch_status")
+        return st
+
+    def download(self, i: int):
+        N = self.models[i].num_nodes
+        x, v = np.empty(3 * N), np.empty(3 * N)
+        self._chk(lib().ms_batch_download_dofs(self._h, i, _dp(x), _dp(v)), "ms_batch_download_dofs")
+        return x, v
+
+    def upload(self, i: int, dofs, vel=None):
+        self._chk(lib().ms_batch_upload_dofs(self._h, i, _dp(_f64(dofs)), _dp(None if vel is None else _f64(vel))),
+                  "ms_batch_upload_dofs")
+
+    def schedule(self) -> dict:
+        s = ms_batch_schedule()
+        self._chk(lib().ms_batch_get_schedule(self._h, C.byref(s)), "ms_batch_get_schedule")
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def set_schedule(self, tri_block: int, node_block: int, chunk_steps: int):
+        s = ms_batch_schedule(tri_block, node_block, chunk_steps)
+        self._chk(lib().ms_batch_set_schedule(self._h, C.byref(s)), "ms_batch_set_schedule")
+
+    def autotune(self, steps_per_trial: int = 20):
+        s = ms_batch_schedule()
+        ms = np.zeros(1)
+        self._chk(lib().ms_batch_autotune(self._h, steps_per_trial, C.byref(s), _dp(ms)), "ms_batch_autotune")
+        return {k: getattr(s, k) for k, _ in s._fields_}, float(ms[0])
+
+    def info(self):
+        N, T, n = C.c_int64(), C.c_int64(), C.c_int32()
+        lib().ms_batch_info(self._h, C.byref(N), C.byref(T), C.byref(n))
+        return {"num_nodes": N.value, "num_tris": T.value, "instances": n.value}
+
+    def stream(self) -> int:
+        return lib().ms_batch_stream(self._h)
+
+
+def run_batch(models, max_steps: int = 0, precision: int = MS_PRECISION_FP64, device: int = -1,
+              stop_at_final_equilibrium: bool = True):
+    """msh_run_batch: the host driver over a batch; returns per-model
+    (msh_run_result, final dofs)."""
+    n = len(models)
+    hs = (C.c_void_p * n)(*[m._h for m in models])
+    o = msh_run_options(max_steps, int(stop_at_final_equilibrium), 0, precision, device, 1, None)
+    res = (msh_run_result * n)()
+    outs = [np.empty(3 * m.num_nodes) for m in models]
+    ptrs = (C.POINTER(C.c_double) * n)(*[_dp(x) for x in outs])
+    rc = lib().msh_run_batch(hs, n, C.byref(o), res, ptrs)
+    if rc != 0:
+        raise RuntimeError(lib().msh_last_error().decode())
+    return [(res[i], outs[i]) for i in range(n)]
 
 
 def device_info() -> str:

@@ -430,6 +430,12 @@ ms_status ms_create(const ms_mesh_desc* d, const ms_params* prm, int device, int
             return bail(MS_ERR_CUDA);
         m.inc_off = doff;
         m.inc_ent = dent;
+        std::vector<int> soff, sent;
+        build_sell(N, off.data(), ent.data(), soff, sent);
+        int *dsoff, *dsent;
+        if ((st = upload(h, &dsoff, soff)) || (st = upload(h, &dsent, sent))) return bail(st);
+        m.sell_off = dsoff;
+        m.sell_ent = dsent;
     }
     // Programmed tensors: flat reference state until ms_set_programmed.
     double *abar, *bbar, *a0, *b0;
@@ -470,19 +476,8 @@ ms_status ms_create(const ms_mesh_desc* d, const ms_params* prm, int device, int
         (st = dalloc(h, &h->d_sum_partial, 1024)) || (st = dalloc(h, &h->d_sums, 4)))
         return bail(st);
     if (precision == MS_PRECISION_MIXED) {
-        float *coef_f, *area_f, *contrib_f;
-        if ((st = dalloc(h, &coef_f, 24ULL * T)) || (st = dalloc(h, &area_f, T)) ||
-            (st = dalloc(h, &contrib_f, 18ULL * T)))
-            return bail(st);
-        std::vector<float> cf(24ULL * T), af(T);
-        for (int t = 0; t < T; ++t) {
-            af[t] = (float)d->ref_area[t];
-            for (int k = 0; k < 24; ++k) cf[(size_t)k * T + t] = (float)d->deriv_coeffs[24ULL * t + k];
-        }
-        cudaMemcpy(coef_f, cf.data(), sizeof(float) * cf.size(), cudaMemcpyHostToDevice);
-        cudaMemcpy(area_f, af.data(), sizeof(float) * T, cudaMemcpyHostToDevice);
-        m.coef_f = coef_f;
-        m.area_f = area_f;
+        float* contrib_f;
+        if ((st = dalloc(h, &contrib_f, 18ULL * T))) return bail(st);
         m.contrib_f = contrib_f;
     }
     h->area_host.assign(d->ref_area, d->ref_area + T);

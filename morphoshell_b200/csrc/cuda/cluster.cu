@@ -73,7 +73,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int ids[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
         const int halo_mask = b.z;
         R f[18];
-        tri_contrib<DIAL, MIXED>(m, p, pos, t, ids, dial, lam, pw, f, m.nu, m.gamma);
+        double h, mu;
+        tri_hmu(m, t, h, mu);
+        tri_contrib<DIAL, MIXED>(m, p, pos, t, ids, dial, lam, pw, f, m.nu, m.gamma, h, mu);
         R* dst = ctr + (size_t)k * kStride;
 #pragma unroll
         for (int j = 0; j < 18; ++j) dst[j] = f[j];
@@ -127,10 +129,16 @@ __global__ void __launch_bounds__(kThreads, 1)
 // Two-kernel path, per-triangle kernel: one thread per triangle over the
 // per-triangle tables (vector loads), all six contributions written to HBM
 // through shared memory as contiguous runs (float for the mixed path).
-constexpr int kAosBlock = 128;
+#ifndef MSB_TRI_BLOCK
+#define MSB_TRI_BLOCK 128
+#endif
+#ifndef MSB_TRI_MINB
+#define MSB_TRI_MINB 1
+#endif
+constexpr int kAosBlock = MSB_TRI_BLOCK;
 
 template <int DIAL, bool MIXED>
-__global__ void __launch_bounds__(kAosBlock)
+__global__ void __launch_bounds__(kAosBlock, MSB_TRI_MINB)
     k_tri_aos(const DevMesh m, const ClusterPlan p, const DevState s, const StepScalars sc) {
     using R = typename Real<MIXED>::T;
     __shared__ R stage[kAosBlock * 18];
@@ -149,7 +157,9 @@ __global__ void __launch_bounds__(kAosBlock)
         const int4 a = __ldg(p.tri_idx + 2 * t);
         const int4 b = __ldg(p.tri_idx + 2 * t + 1);
         const int ids[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
-        tri_contrib<DIAL, MIXED>(m, p, pos_buf(s, sc.parity), t, ids, dial, lam, pw, f, m.nu, m.gamma);
+        double h, mu;
+        tri_hmu(m, t, h, mu);
+        tri_contrib<DIAL, MIXED>(m, p, pos_buf(s, sc.parity), t, ids, dial, lam, pw, f, m.nu, m.gamma, h, mu);
     } else {
 #pragma unroll
         for (int j = 0; j < 18; ++j) f[j] = R(0);

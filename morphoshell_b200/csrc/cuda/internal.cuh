@@ -16,9 +16,13 @@
 //   contrib[T][6][3]             per-(triangle, patch slot) force contribution
 //   inc_off[N+1], inc_ent[6T]    for each node, the (6t+slot) entries that
 //                                touch it, in ascending t (deterministic gather)
+//   sell_off, sell_ent           the same lists in slices of 32 nodes, entry-
+//                                major within a slice (coalesced index loads)
 #pragma once
 
 #include <cstdint>
+#include <vector>
+
 #include <cuda_runtime.h>
 
 namespace msb {
@@ -62,6 +66,12 @@ struct DevMesh {
     const unsigned char* boundary;
     const int* inc_off;
     const int* inc_ent;
+    // The same lists sliced for the node kernel (sliced ELL, 32 nodes a
+    // slice): slice w holds nodes 32w .. 32w+31; its entries start at
+    // sell_off[w], entry k of node 32w+lane is sell_ent[sell_off[w] + 32k +
+    // lane] (ascending t, then -1 padding up to the slice's longest list).
+    const int* sell_off;
+    const int* sell_ent;
     // programmed tensors
     double* abar;
     double* bbar;
@@ -75,9 +85,7 @@ struct DevMesh {
     double h_uniform, mu_uniform;
     // constants
     double nu, gamma;
-    // float copies for the mixed-precision path (may be null)
-    const float* coef_f;
-    const float* area_f;
+    // float contributions of the mixed-precision path (null otherwise)
     float* contrib_f;
 };
 
@@ -115,11 +123,16 @@ struct ClusterPlan {
 // and its own copy of the main loop's state machine (main.cpp:269-508), run
 // on the device so that long stretches need no host round trip.
 struct InstParams {
-    double timestep, damping1, damping2, rho_hh, force_limit, nu, gamma;
+    double dt, damping1, damping2, rho_hh, force_limit;
+    double nu, gamma;
+    double h, mu;                  // used when uniform_hmu
     double char_force, char_speed, force_thresh, speed_thresh;
-    double spacing, lam_final, nu_ot;
+    double spacing;                // dial_factors_to_hold_at_spacing
+    double lam_final, nu_ot;       // protocol-3 field (uniform per instance)
     long long steps_per_phase, steps_between_checks;
-    int node_begin, node_end;
+    int node_begin, node_end;      // union node range
+    int uniform_hmu;
+    int stop_at_final;
 };
 
 enum InstStatus { INST_DIALLING = 0, INST_WAITING = 1, INST_EQUIL = 2, INST_DONE = 3, INST_FAILED = 4 };
@@ -128,21 +141,13 @@ struct InstState {
     int status;
     int check_now;             // this step carries an equilibrium check
     int equilibria;
-    int pad;
-    long long k_phase, since_check, stepcount;
+    int frozen_parity;         // buffer holding a done / failed instance's state, else -1
+    long long k_phase, tsc, stepcount;
     double dial_factor, last_equil_dial, time, damping;
-    double cur_dial, cur_lam, cur_pw;  // dial values of the last dialled step
-    double max_force, max_speed;       // last check
+    double cur_dial, cur_lam, cur_pw;  // protocol-3 values of the last dialled step
+    double max_force, max_speed;       // at the last check
     long long max_force_node, max_speed_node;
-};
-
-struct BatchView {
-    int n_inst;
-    const int* node_inst;      // [N]
-    const InstParams* ip;      // [n_inst]
-    InstState* is;             // [n_inst]
-    double* fnorm;             // [N] |F| on check steps
-    double* vnorm;             // [N] |v| on check steps
+    unsigned long long guard_key;      // smallest tripping dof (within the instance) of this step, ~0 if none
 };
 
 struct DevState {
@@ -175,8 +180,6 @@ struct StepScalars {
 enum DialMode { DIAL_ARRAYS = 0, DIAL_LCE = 3 };
 
 // ---- launchers (kernels.cu) ------------------------------------------------
-cudaError_t launch_tri_fused(const DevMesh& m, const DevState& s, const StepScalars& sc, int dial_mode,
-                             int mixed, cudaStream_t st);
 cudaError_t launch_node_update(const DevMesh& m, const DevState& s, const StepScalars& sc, int mixed,
                                cudaStream_t st);
 cudaError_t launch_surface_derivs(const DevMesh& m, const DevState& s, int parity, cudaStream_t st);
@@ -223,6 +226,9 @@ int cluster_threads();
 // any stream capture).
 cudaError_t prepare_cluster_kernels(int tpc);
 // Deterministic compensated sum of n doubles into *out (two passes, fixed order).
+// Sliced-ELL copy of the incidence lists (see DevMesh::sell_off): offsets
+// [ceil(N/32) + 1] and entries, built on the host from the CSR lists.
+void build_sell(int N, const int* off, const int* ent, std::vector<int>& sell_off, std::vector<int>& sell_ent);
 cudaError_t launch_comp_sum(const double* x, int n, double* partial /*>= 1024*/, double* out, cudaStream_t st);
 
 }  // namespace msb

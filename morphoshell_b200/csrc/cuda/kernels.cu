@@ -1,12 +1,7 @@
 // sm_100a kernels of the force-and-dynamics loop.
 //
-// Fused path, two kernels per step:
-//   k_tri_fused   one thread per triangle: gather the 6 patch nodes, form the
-//                 15 continuum quantities (calc_surface_derivs.cpp:33), the
-//                 energy gradient (calc_deformation_forces.cpp:53-171) and the
-//                 6 per-node force contributions -(D^T dE/dcq) restricted to
-//                 this triangle; protocol-3 dialling (do_dialling.cpp:112-123)
-//                 is evaluated in-line.
+// Fused path, two kernels per step: the per-triangle kernel k_tri_aos
+// (cluster.cu) writes each triangle's 6 per-node force contributions, then
 //   k_node_update one thread per node: deterministic gather of its
 //                 contributions in ascending triangle order (the transposed
 //                 SpMV of calc_deformation_forces.cpp:185), damping
@@ -16,6 +11,7 @@
 //                 symplectic Euler update (advance_dynamics.cpp:58-93).
 // No floating-point atomics anywhere: every sum has a fixed order, so runs
 // are bitwise reproducible.
+#include <algorithm>
 #include <cfloat>
 #include <climits>
 #include <cstdint>
@@ -35,7 +31,6 @@ using namespace stepdev;
 
 namespace {
 
-constexpr int kTriBlock = 128;
 constexpr int kNodeBlock = 256;
 
 template <typename R>
@@ -107,78 +102,6 @@ __device__ __forceinline__ void slot_forces(const R (&coef)[24], const CqGrad<R>
     }
 }
 
-// Write a warp's 32 x 18 contributions through shared memory so that global
-// stores are contiguous 256-byte runs.
-__device__ __forceinline__ void store_contrib_warp(double* __restrict__ out, int t, int T, const double (&f)[18],
-                                                   double* smem_warp) {
-    const int lane = threadIdx.x & 31;
-    const int t0 = t - lane;
-#pragma unroll
-    for (int j = 0; j < 18; ++j) smem_warp[lane * 18 + j] = f[j];
-    __syncwarp();
-    const int nvalid = min(32, T - t0);
-    const int total = nvalid * 18;
-    double* base = out + (size_t)t0 * 18;
-    for (int j = lane; j < total; j += 32) base[j] = smem_warp[j];
-    __syncwarp();
-}
-
-template <int DIAL, bool MIXED>
-__global__ void __launch_bounds__(kTriBlock) k_tri_fused(const DevMesh m, const DevState s, const StepScalars sc) {
-    __shared__ double smem[kTriBlock * 18];
-    const int t = blockIdx.x * kTriBlock + threadIdx.x;
-    const bool live = t < m.T;
-    const int gstep = global_step(s.err, sc.step);
-    if (stale(s.err, gstep)) return;  // uniform across the grid
-    double f[18];
-    if (live) {
-        const double* pos = pos_buf(s, sc.parity);
-        int ids[6];
-#pragma unroll
-        for (int k = 0; k < 6; ++k) ids[k] = __ldg(m.patch + (size_t)k * m.T + t);
-        TriMat<double> mt;
-        load_material(m, t, mt);
-        if (DIAL == DIAL_LCE) {
-            const double dial = s.dials[3 * gstep];
-            dev::lce_abar(dial, __ldg(m.info_a + t), __ldg(m.info_a + (size_t)m.T + t),
-                          __ldg(m.info_a + 2 * (size_t)m.T + t), mt.abar0, mt.abar1, mt.abar2);
-            mt.bbar0 = mt.bbar1 = mt.bbar2 = 0.0;
-        } else {
-            mt.abar0 = __ldg(m.abar + t);
-            mt.abar1 = __ldg(m.abar + (size_t)m.T + t);
-            mt.abar2 = __ldg(m.abar + 2 * (size_t)m.T + t);
-            mt.bbar0 = __ldg(m.bbar + t);
-            mt.bbar1 = __ldg(m.bbar + (size_t)m.T + t);
-            mt.bbar2 = __ldg(m.bbar + 2 * (size_t)m.T + t);
-        }
-        if (!MIXED) {
-            Cq<double> c;
-            double coef[24];
-            load_cq_from_patch<double>(m, pos, t, ids, c, coef);
-            CqGrad<double> g;
-            dev::energy_gradient<double>(c, mt, m.nu, m.gamma, g);
-            slot_forces<double>(coef, g, f);
-        } else {
-            Cq<float> c;
-            float coef[24];
-            load_cq_from_patch<float>(m, pos, t, ids, c, coef);
-            TriMat<float> mf = {(float)mt.abar0, (float)mt.abar1, (float)mt.abar2, (float)mt.bbar0,
-                                (float)mt.bbar1, (float)mt.bbar2, (float)mt.h, (float)mt.mu, (float)mt.area};
-            CqGrad<float> g;
-            dev::energy_gradient<float>(c, mf, (float)m.nu, (float)m.gamma, g);
-            float ff[18];
-            slot_forces<float>(coef, g, ff);
-#pragma unroll
-            for (int j = 0; j < 18; ++j) f[j] = ff[j];
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < 18; ++j) f[j] = 0.0;
-    }
-    const int warp = threadIdx.x >> 5;
-    if (__any_sync(0xffffffffu, live)) store_contrib_warp(s.contrib, t, m.T, f, smem + warp * 32 * 18);
-}
-
 // Block-wide max with first-index tie-break, then the last block to finish
 // folds the per-block partials in block order.
 __device__ __forceinline__ void eq_block_reduce_and_finish(const DevState& s, double fmax, int fnode, double vmax,
@@ -195,41 +118,11 @@ __global__ void __launch_bounds__(kNodeBlock) k_node_update(const DevMesh m, con
     const int N = m.N;
     double fmax = -1.0, vmax = -1.0;
     int fnode = INT_MAX, vnode = INT_MAX;
-    if (n < N) {
-        const int b = __ldg(m.inc_off + n), e = __ldg(m.inc_off + n + 1);
+    if ((n & ~31) < N) {  // warp-uniform; lanes past N walk padding only
         double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-        using Cf = typename std::conditional<MIXED, float, double>::type;
-        const Cf* __restrict__ c;
-        if constexpr (MIXED) c = m.contrib_f;
-        else c = s.contrib;
-        // Indices eight at a time, then all their contributions, so that a
-        // node's loads are in flight together; the sum stays in entry order.
-        int k = b;
-        for (; k + 7 < e; k += 8) {
-            int ei[8];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) ei[j] = __ldg(m.inc_ent + k + j);
-            Cf v[8][3];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                v[j][0] = c[3 * (size_t)ei[j]];
-                v[j][1] = c[3 * (size_t)ei[j] + 1];
-                v[j][2] = c[3 * (size_t)ei[j] + 2];
-            }
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                Fx += (double)v[j][0];
-                Fy += (double)v[j][1];
-                Fz += (double)v[j][2];
-            }
-        }
-        for (; k < e; ++k) {
-            const int e0 = __ldg(m.inc_ent + k);
-            Fx += (double)c[3 * (size_t)e0];
-            Fy += (double)c[3 * (size_t)e0 + 1];
-            Fz += (double)c[3 * (size_t)e0 + 2];
-        }
-        node_finish(m, s, sc, gstep, n, Fx, Fy, Fz, fmax, fnode, vmax, vnode);
+        if constexpr (MIXED) gather_sell<float>(m, m.contrib_f, n, Fx, Fy, Fz);
+        else gather_sell<double>(m, s.contrib, n, Fx, Fy, Fz);
+        if (n < N) node_finish(m, s, sc, gstep, n, Fx, Fy, Fz, fmax, fnode, vmax, vnode);
     }
     if (sc.check) eq_block_reduce_and_finish(s, fmax, fnode, vmax, vnode);
 }
@@ -665,19 +558,6 @@ inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
 }  // namespace
 
-cudaError_t launch_tri_fused(const DevMesh& m, const DevState& s, const StepScalars& sc, int dial_mode, int mixed,
-                             cudaStream_t st) {
-    const int nb = blocks_for(m.T, kTriBlock);
-    if (dial_mode == DIAL_LCE) {
-        if (mixed) k_tri_fused<DIAL_LCE, true><<<nb, kTriBlock, 0, st>>>(m, s, sc);
-        else k_tri_fused<DIAL_LCE, false><<<nb, kTriBlock, 0, st>>>(m, s, sc);
-    } else {
-        if (mixed) k_tri_fused<DIAL_ARRAYS, true><<<nb, kTriBlock, 0, st>>>(m, s, sc);
-        else k_tri_fused<DIAL_ARRAYS, false><<<nb, kTriBlock, 0, st>>>(m, s, sc);
-    }
-    return cudaGetLastError();
-}
-
 cudaError_t launch_node_update(const DevMesh& m, const DevState& s, const StepScalars& sc, int mixed,
                                cudaStream_t st) {
     const int nb = blocks_for(m.N, kNodeBlock);
@@ -753,6 +633,22 @@ cudaError_t launch_comp_sum(const double* x, int n, double* partial, double* out
     k_comp_sum_pass1<<<nb, 256, 0, st>>>(x, n, partial);
     k_comp_sum_pass2<<<1, 1, 0, st>>>(partial, nb, out);
     return cudaGetLastError();
+}
+
+void build_sell(int N, const int* off, const int* ent, std::vector<int>& sell_off, std::vector<int>& sell_ent) {
+    const int W = (N + 31) / 32;
+    sell_off.assign(W + 1, 0);
+    for (int w = 0; w < W; ++w) {
+        int width = 0;
+        for (int l = 0; l < 32 && 32 * w + l < N; ++l) width = std::max(width, off[32 * w + l + 1] - off[32 * w + l]);
+        sell_off[w + 1] = sell_off[w] + 32 * width;
+    }
+    sell_ent.assign((size_t)sell_off[W], -1);
+    for (int w = 0; w < W; ++w)
+        for (int l = 0; l < 32 && 32 * w + l < N; ++l) {
+            const int n = 32 * w + l;
+            for (int k = off[n]; k < off[n + 1]; ++k) sell_ent[(size_t)sell_off[w] + 32 * (k - off[n]) + l] = ent[k];
+        }
 }
 
 }  // namespace msb

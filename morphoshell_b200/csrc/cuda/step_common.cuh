@@ -154,5 +154,48 @@ __device__ __forceinline__ void node_finish(const DevMesh& m, const DevState& s,
     nvel[2 * N + n] = nvz;
 }
 
+// Entries whose indices, then contributions, one thread loads together.
+#ifndef MSB_NODE_BATCH
+#define MSB_NODE_BATCH 8
+#endif
+constexpr int kNodeBatch = MSB_NODE_BATCH;
+
+// Sum of node n's contributions in entry order over the sliced lists: the
+// warp's slice header is one broadcast load, entry indices load coalesced
+// (entry k of the 32 nodes is 128 contiguous bytes), and kNodeBatch
+// indices, then their contributions, are in flight at once.  The loop
+// bound (the slice width) is uniform over the warp.
+template <typename Cf>
+__device__ __forceinline__ void gather_sell(const DevMesh& m, const Cf* __restrict__ c, int n, double& Fx,
+                                            double& Fy, double& Fz) {
+    const int w = n >> 5, lane = n & 31;
+    const int base = __ldg(m.sell_off + w);
+    const int width = (__ldg(m.sell_off + w + 1) - base) >> 5;
+    const int* __restrict__ ep = m.sell_ent + base + lane;
+    for (int k = 0; k < width; k += kNodeBatch) {
+        int ei[kNodeBatch];
+#pragma unroll
+        for (int j = 0; j < kNodeBatch; ++j) ei[j] = (k + j < width) ? __ldg(ep + 32 * (k + j)) : -1;
+        Cf v[kNodeBatch][3];
+#pragma unroll
+        for (int j = 0; j < kNodeBatch; ++j) {
+            if (ei[j] >= 0) {
+                const Cf* q = c + 3 * (size_t)ei[j];
+                v[j][0] = q[0];
+                v[j][1] = q[1];
+                v[j][2] = q[2];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kNodeBatch; ++j) {
+            if (ei[j] >= 0) {
+                Fx += (double)v[j][0];
+                Fy += (double)v[j][1];
+                Fz += (double)v[j][2];
+            }
+        }
+    }
+}
+
 }  // namespace stepdev
 }  // namespace msb

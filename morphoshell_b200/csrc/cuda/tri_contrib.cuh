@@ -21,22 +21,32 @@ struct Real<true> {
     using T = float;
 };
 
+// Thickness and shear modulus of triangle t.
+__device__ __forceinline__ void tri_hmu(const DevMesh& m, int t, double& h, double& mu) {
+    if (m.uniform_hmu) {
+        h = m.h_uniform;
+        mu = m.mu_uniform;
+    } else {
+        h = __ldg(m.thick + t);
+        mu = __ldg(m.shear + t);
+    }
+}
+
 // Contributions of triangle t to its six patch nodes, in the precision of
-// the path (double, or float for the mixed path).
+// the path (double, or float for the mixed path).  With DIAL_LCE the
+// programmed metric is protocol 3 at (dial, lam = lambda, pw = lambda^(-2 nu_ot))
+// over the director trigonometry in p.tri_aux; otherwise it is read from
+// m.abar / m.bbar.
 template <int DIAL, bool MIXED>
 __device__ __forceinline__ void tri_contrib(const DevMesh& m, const ClusterPlan& p, const double* __restrict__ pos,
                                             int t, const int (&ids)[6], double dial, double lam, double pw,
-                                            typename Real<MIXED>::T (&f)[18], double nu, double gamma) {
+                                            typename Real<MIXED>::T (&f)[18], double nu, double gamma, double h,
+                                            double mu) {
     using R = typename Real<MIXED>::T;
     const int N = m.N;
     TriMat<double> mt;
-    if (m.uniform_hmu) {
-        mt.h = m.h_uniform;
-        mt.mu = m.mu_uniform;
-    } else {
-        mt.h = __ldg(m.thick + t);
-        mt.mu = __ldg(m.shear + t);
-    }
+    mt.h = h;
+    mt.mu = mu;
     if (DIAL == DIAL_LCE) {
         const double2* ap = reinterpret_cast<const double2*>(p.tri_aux + t);
         const double2 a01 = __ldg(ap), a23 = __ldg(ap + 1);
@@ -63,27 +73,6 @@ __device__ __forceinline__ void tri_contrib(const DevMesh& m, const ClusterPlan&
         mt.bbar2 = __ldg(m.bbar + 2 * (size_t)m.T + t);
     }
     R c[24];
-    if constexpr (!MIXED) {
-        const double2* cp = reinterpret_cast<const double2*>(p.coef_aos + 24 * (size_t)t);
-#pragma unroll
-        for (int k = 0; k < 12; ++k) {
-            const double2 v = __ldg(cp + k);
-            c[2 * k] = (R)v.x;
-            c[2 * k + 1] = (R)v.y;
-        }
-    } else {
-        const float4* cp = reinterpret_cast<const float4*>(p.coef_aos_f + 24 * (size_t)t);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const float4 v = __ldg(cp + k);
-            c[4 * k] = (R)v.x;
-            c[4 * k + 1] = (R)v.y;
-            c[4 * k + 2] = (R)v.z;
-            c[4 * k + 3] = (R)v.w;
-        }
-    }
-    // Positions; the mixed path works with differences from vertex 0, formed
-    // in double, so the float sums below do not cancel large coordinates.
     double P[6][3];
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
@@ -91,42 +80,94 @@ __device__ __forceinline__ void tri_contrib(const DevMesh& m, const ClusterPlan&
         P[s][1] = __ldg(pos + N + ids[s]);
         P[s][2] = __ldg(pos + 2 * N + ids[s]);
     }
-    R Q[6][3];
-#pragma unroll
-    for (int s = 0; s < 6; ++s)
-#pragma unroll
-        for (int i = 0; i < 3; ++i) Q[s][i] = MIXED ? (R)(P[s][i] - P[0][i]) : (R)P[s][i];
-    R rx[3], ry[3], rxx[3], rxy[3], ryy[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        rx[i] = c[0] * Q[0][i] + c[1] * Q[1][i] + c[2] * Q[2][i];
-        ry[i] = c[3] * Q[0][i] + c[4] * Q[1][i] + c[5] * Q[2][i];
-        R sxx = 0, sxy = 0, syy = 0;
-#pragma unroll
-        for (int s = 0; s < 6; ++s) {
-            sxx += c[6 + 3 * s + 0] * Q[s][i];
-            sxy += c[6 + 3 * s + 1] * Q[s][i];
-            syy += c[6 + 3 * s + 2] * Q[s][i];
-        }
-        rxx[i] = sxx;
-        rxy[i] = sxy;
-        ryy[i] = syy;
-    }
     Cq<R> q;
-    q.rx = {rx[0], rx[1], rx[2]};
-    q.ry = {ry[0], ry[1], ry[2]};
-    q.rxx = {rxx[0], rxx[1], rxx[2]};
-    q.rxy = {rxy[0], rxy[1], rxy[2]};
-    q.ryy = {ryy[0], ryy[1], ryy[2]};
     CqGrad<R> g;
     if constexpr (!MIXED) {
+        const double2* cp = reinterpret_cast<const double2*>(p.coef_aos + 24 * (size_t)t);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            const double2 v = __ldg(cp + k);
+            c[2 * k] = v.x;
+            c[2 * k + 1] = v.y;
+        }
+        double rx[3], ry[3], rxx[3], rxy[3], ryy[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            rx[i] = c[0] * P[0][i] + c[1] * P[1][i] + c[2] * P[2][i];
+            ry[i] = c[3] * P[0][i] + c[4] * P[1][i] + c[5] * P[2][i];
+            double sxx = 0, sxy = 0, syy = 0;
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                sxx += c[6 + 3 * s + 0] * P[s][i];
+                sxy += c[6 + 3 * s + 1] * P[s][i];
+                syy += c[6 + 3 * s + 2] * P[s][i];
+            }
+            rxx[i] = sxx;
+            rxy[i] = sxy;
+            ryy[i] = syy;
+        }
+        q.rx = {rx[0], rx[1], rx[2]};
+        q.ry = {ry[0], ry[1], ry[2]};
+        q.rxx = {rxx[0], rxx[1], rxx[2]};
+        q.rxy = {rxy[0], rxy[1], rxy[2]};
+        q.ryy = {ryy[0], ryy[1], ryy[2]};
         dev::energy_gradient<double>(q, mt, nu, gamma, g);
     } else {
+        // Positions relative to vertex 0, formed in double.  The first
+        // derivatives and the metric a (hence the strain a - abar) are
+        // accumulated in double from the float weights: a is close to abar,
+        // so a float a - abar would be mostly rounding noise that changes
+        // from state to state, while the rounding of the weights only
+        // perturbs the reference triangle by a fixed ~1e-7.  The second
+        // derivatives and everything after the strain are float.
+        const float4* cp = reinterpret_cast<const float4*>(p.coef_aos_f + 24 * (size_t)t);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const float4 v = __ldg(cp + k);
+            c[4 * k] = v.x;
+            c[4 * k + 1] = v.y;
+            c[4 * k + 2] = v.z;
+            c[4 * k + 3] = v.w;
+        }
+        const double dd[6] = {c[0], c[1], c[2], c[3], c[4], c[5]};
+        const float* mw = c + 6;
+        double Q[6][3];
+#pragma unroll
+        for (int s = 1; s < 6; ++s)
+#pragma unroll
+            for (int i = 0; i < 3; ++i) Q[s][i] = P[s][i] - P[0][i];
+        double rx[3], ry[3];
+        float rxx[3], rxy[3], ryy[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            rx[i] = dd[1] * Q[1][i] + dd[2] * Q[2][i];
+            ry[i] = dd[4] * Q[1][i] + dd[5] * Q[2][i];
+            float sxx = 0.f, sxy = 0.f, syy = 0.f;
+#pragma unroll
+            for (int s = 1; s < 6; ++s) {
+                const float qf = (float)Q[s][i];
+                sxx += mw[3 * s + 0] * qf;
+                sxy += mw[3 * s + 1] * qf;
+                syy += mw[3 * s + 2] * qf;
+            }
+            rxx[i] = sxx;
+            rxy[i] = sxy;
+            ryy[i] = syy;
+        }
+        const double a0 = rx[0] * rx[0] + rx[1] * rx[1] + rx[2] * rx[2];
+        const double a1 = rx[0] * ry[0] + rx[1] * ry[1] + rx[2] * ry[2];
+        const double a2 = ry[0] * ry[0] + ry[1] * ry[1] + ry[2] * ry[2];
+        q.rx = {(float)rx[0], (float)rx[1], (float)rx[2]};
+        q.ry = {(float)ry[0], (float)ry[1], (float)ry[2]};
+        q.rxx = {rxx[0], rxx[1], rxx[2]};
+        q.rxy = {rxy[0], rxy[1], rxy[2]};
+        q.ryy = {ryy[0], ryy[1], ryy[2]};
         double sp, bp;
         dev::prefactors<double>(mt, nu, sp, bp);
         const TriMat<float> mf = {(float)mt.abar0, (float)mt.abar1, (float)mt.abar2, (float)mt.bbar0,
                                   (float)mt.bbar1, (float)mt.bbar2, (float)mt.h, (float)mt.mu, (float)mt.area};
-        dev::energy_gradient_pref<float>(q, mf, (float)nu, (float)gamma, (float)sp, (float)bp, g);
+        dev::energy_gradient_strain<float>(q, mf, (float)nu, (float)gamma, (float)sp, (float)bp,
+                                           (float)(a0 - mt.abar0), (float)(a1 - mt.abar1), (float)(a2 - mt.abar2), g);
     }
 #pragma unroll
     for (int s = 0; s < 6; ++s) {

@@ -108,6 +108,10 @@ __device__ __forceinline__ void prefactors(const TriMat<R>& m, R nu, R& sp, R& b
 template <typename R>
 __device__ __forceinline__ void energy_gradient_pref(const Cq<R>& c, const TriMat<R>& m, R nu, R gamma, R sp, R bp,
                                                      CqGrad<R>& g, R* w_stretch = nullptr, R* w_bend = nullptr);
+template <typename R>
+__device__ __forceinline__ void energy_gradient_strain(const Cq<R>& c, const TriMat<R>& m, R nu, R gamma, R sp, R bp,
+                                                       R d0, R d1, R d2, CqGrad<R>& g, R* w_stretch = nullptr,
+                                                       R* w_bend = nullptr);
 
 // Energy gradient of one triangle.  Also returns the stretch and bend
 // (stiffened) energy densities, used by the energy reductions.
@@ -119,15 +123,24 @@ __device__ __forceinline__ void energy_gradient(const Cq<R>& c, const TriMat<R>&
     energy_gradient_pref(c, m, nu, gamma, sp, bp, g, w_stretch, w_bend);
 }
 
-// The same with the prefactors given (the mixed-precision path forms them in
-// double and passes them rounded to float).
+// The same with the prefactors given.
 template <typename R>
 __device__ __forceinline__ void energy_gradient_pref(const Cq<R>& c, const TriMat<R>& m, R nu, R gamma, R sp, R bp,
                                                      CqGrad<R>& g, R* w_stretch, R* w_bend) {
-    // Stretch.
     const R a0 = dot(c.rx, c.rx), a1 = dot(c.rx, c.ry), a2 = dot(c.ry, c.ry);
+    energy_gradient_strain(c, m, nu, gamma, sp, bp, a0 - m.abar0, a1 - m.abar1, a2 - m.abar2, g, w_stretch, w_bend);
+}
+
+// The same with the stretch strain d = a - abar given.  The mixed-precision
+// path forms d in double (a ~ 1 while d is small, so a float a - abar would
+// lose most of d's digits) and the prefactors in double, and runs the rest in
+// float.
+template <typename R>
+__device__ __forceinline__ void energy_gradient_strain(const Cq<R>& c, const TriMat<R>& m, R nu, R gamma, R sp, R bp,
+                                                       R d0, R d1, R d2, CqGrad<R>& g, R* w_stretch, R* w_bend) {
+    // Stretch.
     R qs0, qs1, qs2;
-    const R ws = quad_form(m.abar0, m.abar1, m.abar2, a0 - m.abar0, a1 - m.abar1, a2 - m.abar2, nu, qs0, qs1, qs2);
+    const R ws = quad_form(m.abar0, m.abar1, m.abar2, d0, d1, d2, nu, qs0, qs1, qs2);
     // dW_s/da_k = sp * q_k.
     const R s0 = sp * qs0, s1 = sp * qs1, s2 = sp * qs2;
 

@@ -295,7 +295,8 @@ int msh_get_boundary(const msh_model* m, uint8_t* b) {
 // decision go to the fused GPU stepper (ms_step_n); steps that check for
 // equilibrium or write output go through the one-call-per-function path so
 // that the check and the output see the state before the update, as in the
-// reference.
+// reference.  With the mixed-precision path a check step is one fused step
+// instead, so that equilibrium is judged on the forces that path steps with.
 int msh_run(msh_model* model, const msh_run_options* opts, msh_run_result* res, double* dofs_out) {
     if (!model || !opts || !res) return set_err("null argument");
     std::memset(res, 0, sizeof(*res));
@@ -349,13 +350,45 @@ int msh_run(msh_model* model, const msh_run_options* opts, msh_run_result* res, 
             "ms_set_programmed");
         log << "Beginning dynamics loop." << std::endl;
 
-        auto write_out = [&](long long step) {
+        // Output quantities of the current state, then the files.
+        auto snap_out = [&]() {
             gpu(ms_output_quantities(h, curv.data(), edens.data(), strains.data(), stresses.data(), deficits.data(),
                                      energies),
                 "ms_output_quantities");
             gpu(ms_download_dofs(h, dofs.data(), nullptr), "ms_download_dofs");
+        };
+        auto emit_out = [&](long long step) {
             if (opts->write_outputs && opts->output_dir)
                 write_output(dofs, model->tris, (int)step, dial_factor, curv, edens, deficits, stresses, strains, st);
+        };
+        auto write_out = [&](long long step) {
+            snap_out();
+            emit_out(step);
+        };
+        auto log_check = [&](const ms_equil_result& eq) {
+            res->last_max_force_ratio = eq.max_force / st.char_force_scale;
+            res->last_max_speed_ratio = eq.max_speed / st.char_speed_scale;
+            log << "Max ratio of non-damping force to characteristic force = " << res->last_max_force_ratio
+                << " (node " << eq.max_force_node << ")" << "\n";
+            log << "Max ratio of node speed to characteristic speed = " << res->last_max_speed_ratio << " (node "
+                << eq.max_speed_node << ")" << "\n";
+            if (eq.at_equilibrium) {
+                st.status = equil_reached;
+                res->equilibria_reached += 1;
+                log << "Equilibrium reached. Writing VTK output at " << get_real_time() << ", stepcount = "
+                    << stepcount << ", simulation time = " << time << ", dial_factor = " << dial_factor << std::endl;
+                last_equil_dial = dial_factor;
+            }
+            tsc = 0;
+        };
+        auto crash = [&](long long dof, double force) {
+            log << " ------------CRASH REPORT-----------------" << std::endl;
+            log << "Offending dof is " << dof << std::endl;
+            log << "Offending force is " << force << std::endl;
+            log << "Offending node is " << dof % N << std::endl;
+            write_out(stepcount);
+            log << "At stepcount = " << stepcount << ", dial_factor = " << dial_factor
+                << " there was a problem: implausibly_high_force" << std::endl;
         };
 
         for (;;) {
@@ -423,13 +456,7 @@ int msh_run(msh_model* model, const msh_run_options* opts, msh_run_result* res, 
                             if (!dialling_now) ++tsc;
                         }
                         if (dialling_now) dial_factor = dials[rep.steps_done];
-                        log << " ------------CRASH REPORT-----------------" << std::endl;
-                        log << "Offending dof is " << rep.offending_dof << std::endl;
-                        log << "Offending force is " << rep.offending_force << std::endl;
-                        log << "Offending node is " << rep.offending_dof % N << std::endl;
-                        write_out(stepcount);
-                        log << "At stepcount = " << stepcount << ", dial_factor = " << dial_factor
-                            << " there was a problem: implausibly_high_force" << std::endl;
+                        crash(rep.offending_dof, rep.offending_force);
                         break;
                     }
                     gpu(code, "ms_step_n");
@@ -445,56 +472,58 @@ int msh_run(msh_model* model, const msh_run_options* opts, msh_run_result* res, 
                     continue;
                 }
             }
-            // One step through the per-function path (main.cpp:308-474).
-            gpu(ms_surface_derivs(h, nullptr), "calc_surface_derivs");
-            if (stepcount == 0 && st.dialling_from_ansatz_rather_than_ref_state) {
-                std::vector<double> a(3ULL * T), b(3ULL * T), nn(3ULL * T);
-                gpu(ms_a_b_normals(h, a.data(), b.data(), nn.data()), "calc_a_comps_and_b_comps_and_normals");
-                gpu(ms_set_zero_dial_state(h, a.data(), b.data()), "ms_set_zero_dial_state");
-            }
-            if (st.status == dialling || stepcount == 0) gpu(ms_do_dialling(h, dial_factor), "do_dialling");
-            gpu(ms_deformation_forces(h, nullptr, nullptr), "calc_deformation_forces");
-            gpu(ms_non_deformation_forces(h, st.damping_factor, st.using_gradient_descent_dynamics), "calc_non_deformation_forces");
-            gpu(ms_impose_constraints(h), "impose_constraints");
-            if (check) {
+            if (check && opts->precision == MS_PRECISION_MIXED) {
+                // The mixed-precision path judges equilibrium in its own
+                // force field (float per-triangle arithmetic, double node
+                // sums): one fused step that also reduces |F| and |v| of
+                // the state before its update (is_at_equilibrium.cpp:62-84).
+                const bool outputs = opts->write_outputs && opts->output_dir;
+                if (outputs) snap_out();
                 log << "Checking for equilibrium at " << get_real_time() << ", stepcount = " << stepcount
                     << ", simulation time = " << time << ", dial_factor = " << dial_factor << std::endl;
-                ms_equil_result eq;
-                gpu(ms_is_at_equilibrium(h, &eq), "is_at_equilibrium");
-                res->last_max_force_ratio = eq.max_force / st.char_force_scale;
-                res->last_max_speed_ratio = eq.max_speed / st.char_speed_scale;
-                log << "Max ratio of non-damping force to characteristic force = " << res->last_max_force_ratio
-                    << " (node " << eq.max_force_node << ")" << "\n";
-                log << "Max ratio of node speed to characteristic speed = " << res->last_max_speed_ratio << " (node "
-                    << eq.max_speed_node << ")" << "\n";
-                if (eq.at_equilibrium) {
-                    st.status = equil_reached;
-                    res->equilibria_reached += 1;
-                    log << "Equilibrium reached. Writing VTK output at " << get_real_time() << ", stepcount = "
-                        << stepcount << ", simulation time = " << time << ", dial_factor = " << dial_factor
-                        << std::endl;
-                    last_equil_dial = dial_factor;
+                ms_step_report rep;
+                code = ms_step_n(h, 1, nullptr, 0, st.timestep, st.damping_factor,
+                                 st.using_gradient_descent_dynamics ? 1 : 0, 1, &rep);
+                if (code == MS_ERR_IMPLAUSIBLE_FORCE) {
+                    crash(rep.offending_dof, rep.offending_force);
+                    break;
                 }
-                tsc = 0;
+                gpu(code, "ms_step_n");
+                log_check(rep.equil);
+                if (outputs && (regular_out || st.status == equil_reached)) emit_out(stepcount);
+            } else {
+                // One step through the per-function path (main.cpp:308-474).
+                gpu(ms_surface_derivs(h, nullptr), "calc_surface_derivs");
+                if (stepcount == 0 && st.dialling_from_ansatz_rather_than_ref_state) {
+                    std::vector<double> a(3ULL * T), b(3ULL * T), nn(3ULL * T);
+                    gpu(ms_a_b_normals(h, a.data(), b.data(), nn.data()), "calc_a_comps_and_b_comps_and_normals");
+                    gpu(ms_set_zero_dial_state(h, a.data(), b.data()), "ms_set_zero_dial_state");
+                }
+                if (st.status == dialling || stepcount == 0) gpu(ms_do_dialling(h, dial_factor), "do_dialling");
+                gpu(ms_deformation_forces(h, nullptr, nullptr), "calc_deformation_forces");
+                gpu(ms_non_deformation_forces(h, st.damping_factor, st.using_gradient_descent_dynamics),
+                    "calc_non_deformation_forces");
+                gpu(ms_impose_constraints(h), "impose_constraints");
+                if (check) {
+                    log << "Checking for equilibrium at " << get_real_time() << ", stepcount = " << stepcount
+                        << ", simulation time = " << time << ", dial_factor = " << dial_factor << std::endl;
+                    ms_equil_result eq;
+                    gpu(ms_is_at_equilibrium(h, &eq), "is_at_equilibrium");
+                    log_check(eq);
+                }
+                if (regular_out || st.status == equil_reached) {
+                    if (opts->write_outputs) write_out(stepcount);
+                }
+                int64_t bad_dof = -1;
+                double bad_force = 0.0;
+                code = ms_advance_dynamics(h, st.timestep, st.damping_factor, st.using_gradient_descent_dynamics,
+                                           &bad_dof, &bad_force);
+                if (code == MS_ERR_IMPLAUSIBLE_FORCE) {
+                    crash(bad_dof, bad_force);
+                    break;
+                }
+                gpu(code, "advance_dynamics");
             }
-            if (regular_out || st.status == equil_reached) {
-                if (opts->write_outputs) write_out(stepcount);
-            }
-            int64_t bad_dof = -1;
-            double bad_force = 0.0;
-            code = ms_advance_dynamics(h, st.timestep, st.damping_factor, st.using_gradient_descent_dynamics, &bad_dof,
-                                       &bad_force);
-            if (code == MS_ERR_IMPLAUSIBLE_FORCE) {
-                log << " ------------CRASH REPORT-----------------" << std::endl;
-                log << "Offending dof is " << bad_dof << std::endl;
-                log << "Offending force is " << bad_force << std::endl;
-                log << "Offending node is " << bad_dof % N << std::endl;
-                write_out(stepcount);
-                log << "At stepcount = " << stepcount << ", dial_factor = " << dial_factor
-                    << " there was a problem: implausibly_high_force" << std::endl;
-                break;
-            }
-            gpu(code, "advance_dynamics");
             time += st.timestep;
             stepcount += 1;
             if (st.status == dialling) k_phase += 1;
@@ -530,6 +559,81 @@ int msh_run(msh_model* model, const msh_run_options* opts, msh_run_result* res, 
     if (res->final_status == 0) res->final_status = st.status;
     res->wall_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
     return code == MS_OK ? 0 : set_err("implausibly_high_force");
+}
+
+// Many models through one ms_batch: each keeps the state machine of
+// msh_run (main.cpp:269-508) on the device.  Supports what the batch
+// supports: protocol 3 without ansatz dialling, Newtonian dynamics, no
+// regular output.
+int msh_run_batch(msh_model* const* models, int32_t n, const msh_run_options* opts, msh_run_result* results,
+                  double* const* dofs_out) {
+    if (!models || n <= 0 || !opts || !results) return set_err("null argument");
+    if (opts->max_steps <= 0 && !opts->stop_at_final_equilibrium)
+        return set_err("msh_run_batch needs max_steps > 0 or stop_at_final_equilibrium");
+    auto wall0 = std::chrono::steady_clock::now();
+    std::vector<ms_batch_instance> inst(n);
+    std::vector<std::vector<double>> info(n), dofs(n);
+    for (int i = 0; i < n; ++i) {
+        msh_model* m = models[i];
+        if (!m) return set_err("null model");
+        const Stuff& st = m->stuff;
+        if (st.dialling_protocol != 3 || st.dialling_from_ansatz_rather_than_ref_state || m->abar_info.cols < 3)
+            return set_err("msh_run_batch: model " + std::to_string(i) +
+                           " is not protocol-3 dialling from the reference state");
+        if (st.using_gradient_descent_dynamics)
+            return set_err("msh_run_batch: model " + std::to_string(i) + " uses gradient-descent steps");
+        const int T = st.num_tris, N = st.num_nodes;
+        info[i].resize(3ULL * T);
+        for (int t = 0; t < T; ++t)
+            for (int k = 0; k < 3; ++k) info[i][3ULL * t + k] = m->abar_info(t, k);
+        dofs[i].resize(3ULL * N);
+        soa_from(m->init_positions, dofs[i].data());
+        ms_batch_instance& b = inst[i];
+        std::memset(&b, 0, sizeof(b));
+        msh_get_desc(m, &b.mesh, &b.params);
+        b.abar_info = info[i].data();
+        b.timestep = st.timestep;
+        b.damping_factor_1 = m->damping_factor_1;
+        b.damping_factor_2 = m->damping_factor_2;
+        b.timesteps_per_dial_phase = st.timesteps_per_dial_phase;
+        b.timesteps_between_equil_checks = st.timesteps_between_equil_checks;
+        b.dial_factors_to_hold_at_spacing = st.dial_factors_to_hold_at_spacing;
+        b.dial_factor_to_start_from = m->dial_factor_to_start_from;
+        b.stop_at_final_equilibrium = opts->stop_at_final_equilibrium ? 1 : 0;
+        b.dofs = dofs[i].data();
+        b.velocities = nullptr;
+    }
+    ms_batch* batch = nullptr;
+    int rc = ms_batch_create(inst.data(), n, opts->device, opts->precision, &batch);
+    if (rc != MS_OK) return set_err(std::string("ms_batch_create failed: ") + ms_status_string(rc));
+    std::unique_ptr<ms_batch, decltype(&ms_batch_destroy)> guard(batch, &ms_batch_destroy);
+    int64_t done = 0;
+    rc = ms_batch_run(batch, opts->max_steps > 0 ? opts->max_steps : INT64_MAX / 2, &done);
+    if (rc != MS_OK) return set_err(std::string("ms_batch_run: ") + ms_batch_last_error(batch));
+    const double wall = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
+    for (int i = 0; i < n; ++i) {
+        ms_batch_inst_status bs;
+        rc = ms_batch_status(batch, i, &bs);
+        if (rc != MS_OK) return set_err(std::string("ms_batch_status: ") + ms_batch_last_error(batch));
+        msh_run_result& r = results[i];
+        std::memset(&r, 0, sizeof(r));
+        r.status = bs.status == MS_INST_FAILED ? MS_ERR_IMPLAUSIBLE_FORCE : MS_OK;
+        r.steps = bs.stepcount;
+        r.final_dial_factor = bs.dial_factor;
+        r.sim_time = bs.sim_time;
+        r.equilibria_reached = bs.equilibria;
+        r.final_status = bs.status == MS_INST_DONE      ? equil_reached
+                         : bs.status == MS_INST_WAITING ? waiting_for_equil
+                                                        : dialling;
+        r.wall_seconds = wall;
+        r.last_max_force_ratio = bs.max_force_ratio;
+        r.last_max_speed_ratio = bs.max_speed_ratio;
+        if (dofs_out && dofs_out[i]) {
+            rc = ms_batch_download_dofs(batch, i, dofs_out[i], nullptr);
+            if (rc != MS_OK) return set_err(std::string("ms_batch_download_dofs: ") + ms_batch_last_error(batch));
+        }
+    }
+    return 0;
 }
 
 }  // extern "C"

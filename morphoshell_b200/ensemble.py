@@ -80,3 +80,46 @@ def run_instances(make_instance, num_instances: int, steps: int, dist=None, weig
         else:
             results = None
     return results, total
+
+
+def _member_arrays(args):
+    from . import meshgen
+    k, seed, spacing_range = args
+    mesh, info, bbar, over, params = meshgen.ensemble_member(k, seed=seed, spacing_range=spacing_range)
+    return mesh.nodes, mesh.tris, info, bbar, over, params
+
+
+def build_members(indices, directory: str, seed: int = 7, spacing_range=(0.004, 0.02), threads: int = 8,
+                  processes: int = 0, **settings):
+    """Host set-up (Model.from_arrays) of the batched-ensemble members
+    ``indices`` (meshgen.ensemble_member).  Meshes are generated in
+    ``processes`` spawned worker processes (0: in the calling process) and
+    set up in ``threads`` threads (the native set-up releases the GIL).
+    Extra keyword arguments override settings of every member.  Returns
+    (models, parameters)."""
+    import multiprocessing as mp
+    import os
+    from concurrent.futures import ProcessPoolExecutor, ThreadPoolExecutor
+
+    from . import Model, meshgen
+
+    os.makedirs(directory, exist_ok=True)
+    jobs = [(k, seed, spacing_range) for k in indices]
+    if processes > 0:
+        with ProcessPoolExecutor(max_workers=processes, mp_context=mp.get_context("spawn")) as ex:
+            arrays = list(ex.map(_member_arrays, jobs))
+    else:
+        with ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
+            arrays = list(ex.map(_member_arrays, jobs))
+
+    def one(item):
+        k, (nodes, tris, info, bbar, over, params) = item
+        st = os.path.join(directory, "member%05d_settings.txt" % k)
+        meshgen.write_settings(st, protocol=3, **dict(over, **settings))
+        model = Model.from_arrays(st, nodes, tris, info, bbar, quiet=True, noise=True)
+        params = dict(params, num_tris=model.num_tris)
+        return model, params
+
+    with ThreadPoolExecutor(max_workers=max(1, threads)) as ex:
+        out = list(ex.map(one, zip(list(indices), arrays)))
+    return [m for m, _ in out], [p for _, p in out]

@@ -293,6 +293,32 @@ def write_settings(path: str, protocol: int | None = 3, **overrides) -> None:
             f.write("dialling_protocol = %d;\n" % protocol)
 
 
+def ensemble_member(k: int, seed: int = 7, spacing_range=(0.004, 0.02)):
+    """Member k of the batched-ensemble workload: mesh spacing log-uniform
+    over ``spacing_range``, lambda_final ~ U(0.8, 1.2), defect charge drawn
+    from {+1, -1, +1/2} with director angle = charge * theta, thickness
+    ~ U(0.005, 0.02), b-bar = 0.  Deterministic in (seed, k).  Returns
+    (mesh, abar_info, bbar_info, settings overrides, parameters)."""
+    params = ensemble_params(k, seed, spacing_range)
+    mesh = disk_mesh(params["spacing"], seed=params["mesh_seed"])
+    charge = params["charge"]
+    info = lce_abar_info(mesh, lambda th, r: charge * th, params["lam_final"])
+    bbar = np.zeros((mesh.num_tris, 3))
+    return mesh, info, bbar, {"ref_thickness_if_uniform": params["thickness"]}, params
+
+
+def ensemble_params(k: int, seed: int = 7, spacing_range=(0.004, 0.02)) -> dict:
+    """The random draws of ensemble_member k, without building its mesh."""
+    rng = np.random.default_rng([seed, k])
+    lo, hi = spacing_range
+    spacing = float(np.exp(rng.uniform(math.log(lo), math.log(hi))))
+    lam = float(rng.uniform(0.8, 1.2))
+    charge = (1.0, -1.0, 0.5)[int(rng.integers(3))]
+    h = float(rng.uniform(0.005, 0.02))
+    return {"spacing": spacing, "lam_final": lam, "charge": charge, "thickness": h,
+            "mesh_seed": int(rng.integers(1 << 31))}
+
+
 def write_workload(directory: str, name: str, seed: int = 1, protocol: int = 3, **settings):
     """Write ``<name>.vtk`` and ``<name>_settings.txt`` into directory and
     return their paths."""
