@@ -292,6 +292,12 @@ ms_status ms_batch_download_dofs(ms_batch* b, int32_t instance, double* dofs, do
 /* Replaces one instance's positions (and velocities; NULL = zero), e.g. a
  * warm start, and restarts its state machine from dial_factor_to_start_from. */
 ms_status ms_batch_upload_dofs(ms_batch* b, int32_t instance, const double* dofs, const double* velocities);
+/* Restarts one instance's state machine at dial_factor: dialling from there
+ * (waiting = 0, as dial_factor_to_start_from), or waiting for equilibrium
+ * with the programmed metric held at dial_factor (waiting = 1; for a warm
+ * start uploaded with ms_batch_upload_dofs, which itself restarts from
+ * dial_factor_to_start_from, so call this after it). */
+ms_status ms_batch_set_start(ms_batch* b, int32_t instance, double dial_factor, int32_t waiting);
 ms_status ms_batch_set_schedule(ms_batch* b, const ms_batch_schedule* s);
 ms_status ms_batch_get_schedule(const ms_batch* b, ms_batch_schedule* s);
 /* Times every built-in schedule on this batch (steps_per_trial steps each,
@@ -301,6 +307,37 @@ ms_status ms_batch_autotune(ms_batch* b, int32_t steps_per_trial, ms_batch_sched
                             double* best_ms_per_step);
 ms_status ms_batch_info(const ms_batch* b, int64_t* num_nodes, int64_t* num_tris, int32_t* n_instances);
 void* ms_batch_stream(ms_batch* b);
+
+/* ---- coordinate network of the learned warm start ---------------------------
+ * No reference counterpart: it replaces move_nodes_to_ansatz_positions
+ * (main.cpp:226-230) as the source of an ansatz.  A SiLU MLP
+ * in_dim -> width (x hidden_layers) -> out_dim; every layer runs on the
+ * tensor cores (tcgen05, BF16 operands, FP32 accumulation); FP32 master
+ * weights, Adam (beta 0.9 / 0.999, eps 1e-8), mean-squared-error loss.
+ * Parameter layout (ms_mlp_get_params): per layer W [N][K] row-major, then
+ * b [Np]; K is in_dim rounded up to 16 for the first layer (the extra
+ * columns stay zero) and width after; N = width, or out_dim for the last
+ * layer whose bias is padded to Np = 16. */
+typedef struct ms_mlp ms_mlp;
+
+ms_status ms_mlp_create(int32_t in_dim, int32_t width, int32_t hidden_layers, int32_t out_dim, uint64_t seed,
+                        int32_t device, ms_mlp** out);
+void ms_mlp_destroy(ms_mlp* h);
+const char* ms_mlp_last_error(const ms_mlp* h);
+ms_status ms_mlp_num_params(const ms_mlp* h, int64_t* n);
+ms_status ms_mlp_get_params(ms_mlp* h, float* params);
+ms_status ms_mlp_set_params(ms_mlp* h, const float* params);
+/* y (n x out_dim) = network(x (n x in_dim)), host arrays, row-major. */
+ms_status ms_mlp_forward(ms_mlp* h, const float* x, int64_t n, float* y);
+/* Mean-squared-error loss of one batch (n <= 65536) and its gradient with
+ * respect to every parameter (ms_mlp_get_params layout); no update. */
+ms_status ms_mlp_loss_grad(ms_mlp* h, const float* x, const float* t, int64_t n, double* loss, float* grads);
+/* Training set (n rows of in_dim inputs and out_dim targets) to the device. */
+ms_status ms_mlp_set_data(ms_mlp* h, const float* x, const float* t, int64_t n);
+/* epochs passes over the training set in shuffled batches of `batch` rows;
+ * epoch_loss (epochs entries, may be NULL) gets each epoch's mean loss. */
+ms_status ms_mlp_train(ms_mlp* h, int32_t epochs, int32_t batch, double lr, uint64_t seed, float* epoch_loss);
+void* ms_mlp_stream(ms_mlp* h);
 
 #ifdef __cplusplus
 }

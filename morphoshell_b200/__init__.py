@@ -30,7 +30,9 @@ GPU_SYMBOLS = [
     "ms_deformation_forces_noalloc", "ms_set_step_path", "ms_plan_info",
     "ms_batch_create", "ms_batch_destroy", "ms_batch_last_error", "ms_batch_run", "ms_batch_status",
     "ms_batch_download_dofs", "ms_batch_upload_dofs", "ms_batch_set_schedule", "ms_batch_get_schedule",
-    "ms_batch_autotune", "ms_batch_info", "ms_batch_stream",
+    "ms_batch_autotune", "ms_batch_info", "ms_batch_stream", "ms_batch_set_start",
+    "ms_mlp_create", "ms_mlp_destroy", "ms_mlp_last_error", "ms_mlp_num_params", "ms_mlp_get_params",
+    "ms_mlp_set_params", "ms_mlp_forward", "ms_mlp_loss_grad", "ms_mlp_set_data", "ms_mlp_train", "ms_mlp_stream",
 ]
 HOST_SYMBOLS = [
     "msh_load", "msh_build", "msh_free", "msh_last_error", "msh_get_scalars", "msh_get_desc", "msh_get_dofs",
@@ -173,12 +175,29 @@ def lib() -> C.CDLL:
         L.ms_batch_download_dofs.argtypes = [C.c_void_p, C.c_int32, d, d]
         L.ms_batch_upload_dofs.argtypes = [C.c_void_p, C.c_int32, d, d]
         L.ms_batch_set_schedule.argtypes = [C.c_void_p, P(ms_batch_schedule)]
+        L.ms_batch_set_start.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_int32]
         L.ms_batch_get_schedule.argtypes = [C.c_void_p, P(ms_batch_schedule)]
         L.ms_batch_autotune.argtypes = [C.c_void_p, C.c_int32, P(ms_batch_schedule), d]
         i64p = C.POINTER(C.c_int64)
         L.ms_batch_info.argtypes = [C.c_void_p, i64p, i64p, P(C.c_int32)]
         L.ms_batch_stream.argtypes = [C.c_void_p]
         L.ms_batch_stream.restype = C.c_void_p
+        fp = C.POINTER(C.c_float)
+        L.ms_mlp_create.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.c_int32,
+                                    P(C.c_void_p)]
+        L.ms_mlp_destroy.argtypes = [C.c_void_p]
+        L.ms_mlp_destroy.restype = None
+        L.ms_mlp_last_error.argtypes = [C.c_void_p]
+        L.ms_mlp_last_error.restype = C.c_char_p
+        L.ms_mlp_num_params.argtypes = [C.c_void_p, i64p]
+        L.ms_mlp_get_params.argtypes = [C.c_void_p, fp]
+        L.ms_mlp_set_params.argtypes = [C.c_void_p, fp]
+        L.ms_mlp_forward.argtypes = [C.c_void_p, fp, C.c_int64, fp]
+        L.ms_mlp_loss_grad.argtypes = [C.c_void_p, fp, fp, C.c_int64, d, fp]
+        L.ms_mlp_set_data.argtypes = [C.c_void_p, fp, fp, C.c_int64]
+        L.ms_mlp_train.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.c_uint64, fp]
+        L.ms_mlp_stream.argtypes = [C.c_void_p]
+        L.ms_mlp_stream.restype = C.c_void_p
         L.msh_run_batch.argtypes = [P(C.c_void_p), C.c_int32, P(msh_run_options), P(msh_run_result),
                                     P(C.POINTER(C.c_double))]
         L.msh_load.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, P(C.c_void_p)]
@@ -447,14 +466,19 @@ class Batch:
     include/morphoshell_gpu.h."""
 
     def __init__(self, models, precision: int = MS_PRECISION_FP64, device: int = -1, dofs=None,
-                 stop_at_final_equilibrium: bool = True):
+                 stop_at_final_equilibrium: bool = True, abar_infos=None):
+        """``models`` may repeat one Model (a shared mesh); ``abar_infos[i]``
+        (T x 3, optional) then gives instance i its own protocol-3 field."""
         L = lib()
         n = len(models)
         arr = (ms_batch_instance * n)()
         self._keep = []
         for i, m in enumerate(models):
             s = m.scalars
-            a_info, _ = m.programmed()
+            if abar_infos is not None and abar_infos[i] is not None:
+                a_info = np.asarray(abar_infos[i], dtype=np.float64)
+            else:
+                a_info, _ = m.programmed()
             if a_info.shape[1] < 3:
                 raise ValueError("instance %d: protocol-3 abar_info needs 3 columns" % i)
             info = np.ascontiguousarray(a_info[:, :3], dtype=np.float64)
@@ -514,6 +538,9 @@ class Batch:
         self._chk(lib().ms_batch_upload_dofs(self._h, i, _dp(_f64(dofs)), _dp(None if vel is None else _f64(vel))),
                   "ms_batch_upload_dofs")
 
+    def set_start(self, i: int, dial_factor: float, waiting: bool):
+        self._chk(lib().ms_batch_set_start(self._h, i, dial_factor, int(waiting)), "ms_batch_set_start")
+
     def schedule(self) -> dict:
         s = ms_batch_schedule()
         self._chk(lib().ms_batch_get_schedule(self._h, C.byref(s)), "ms_batch_get_schedule")
@@ -536,6 +563,92 @@ class Batch:
 
     def stream(self) -> int:
         return lib().ms_batch_stream(self._h)
+
+
+def _fp(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Mlp:
+    """The warm-start coordinate network (ms_mlp_*): SiLU MLP on the tensor
+    cores, BF16 operands, FP32 accumulation and master weights, Adam."""
+
+    def __init__(self, in_dim: int, width: int = 256, hidden_layers: int = 4, out_dim: int = 3, seed: int = 0,
+                 device: int = -1):
+        h = C.c_void_p()
+        rc = lib().ms_mlp_create(in_dim, width, hidden_layers, out_dim, seed, device, C.byref(h))
+        if rc != MS_OK:
+            raise MsError(rc, "ms_mlp_create: %s" % lib().ms_status_string(rc).decode())
+        self._h = h
+        self.in_dim, self.width, self.hidden_layers, self.out_dim = in_dim, width, hidden_layers, out_dim
+        self.in_pad = (in_dim + 15) // 16 * 16
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ms_mlp_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def _chk(self, rc, what):
+        if rc != MS_OK:
+            raise MsError(rc, "%s: %s (%s)" % (what, lib().ms_status_string(rc).decode(),
+                                                lib().ms_mlp_last_error(self._h).decode()))
+
+    def num_params(self) -> int:
+        n = C.c_int64()
+        self._chk(lib().ms_mlp_num_params(self._h, C.byref(n)), "ms_mlp_num_params")
+        return n.value
+
+    def params(self) -> np.ndarray:
+        p = np.empty(self.num_params(), dtype=np.float32)
+        self._chk(lib().ms_mlp_get_params(self._h, _fp(p)), "ms_mlp_get_params")
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.num_params()
+        self._chk(lib().ms_mlp_set_params(self._h, _fp(p)), "ms_mlp_set_params")
+
+    def layers(self):
+        """[(W [N][K], b [Np]) views into a params() vector's layout]: (offset, N, K, Np) per layer."""
+        out, off = [], 0
+        nl = self.hidden_layers + 1
+        for l in range(nl):
+            K = self.in_pad if l == 0 else self.width
+            N = self.out_dim if l == nl - 1 else self.width
+            Np = 16 if l == nl - 1 else self.width
+            out.append((off, N, K, Np))
+            off += N * K + Np
+        return out
+
+    def forward(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        y = np.empty((x.shape[0], self.out_dim), dtype=np.float32)
+        self._chk(lib().ms_mlp_forward(self._h, _fp(x), x.shape[0], _fp(y)), "ms_mlp_forward")
+        return y
+
+    def loss_grad(self, x, t):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.empty(self.num_params(), dtype=np.float32)
+        loss = np.zeros(1)
+        self._chk(lib().ms_mlp_loss_grad(self._h, _fp(x), _fp(t), x.shape[0], _dp(loss), _fp(g)),
+                  "ms_mlp_loss_grad")
+        return float(loss[0]), g
+
+    def set_data(self, x, t):
+        self._x = np.ascontiguousarray(x, dtype=np.float32)
+        self._t = np.ascontiguousarray(t, dtype=np.float32)
+        self._chk(lib().ms_mlp_set_data(self._h, _fp(self._x), _fp(self._t), self._x.shape[0]), "ms_mlp_set_data")
+
+    def train(self, epochs: int, batch: int = 8192, lr: float = 1e-3, seed: int = 0) -> np.ndarray:
+        losses = np.zeros(epochs, dtype=np.float32)
+        self._chk(lib().ms_mlp_train(self._h, epochs, batch, lr, seed, _fp(losses)), "ms_mlp_train")
+        return losses
+
+    def stream(self) -> int:
+        return lib().ms_mlp_stream(self._h)
 
 
 def run_batch(models, max_steps: int = 0, precision: int = MS_PRECISION_FP64, device: int = -1,

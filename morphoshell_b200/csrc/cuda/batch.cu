@@ -724,6 +724,32 @@ ms_status ms_batch_upload_dofs(ms_batch* b, int32_t i, const double* dofs, const
     return MS_OK;
 }
 
+ms_status ms_batch_set_start(ms_batch* b, int32_t i, double dial_factor, int32_t waiting) {
+    if (!b || i < 0 || i >= b->n_inst || !(dial_factor >= 0.0) || dial_factor > 1.0) return MS_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(b->device);
+    MB_CUDA(b, cudaStreamSynchronize(b->stream));
+    const InstParams& q = b->ip[i];
+    InstState st = b->init_state[i];
+    st.dial_factor = st.last_equil_dial = dial_factor;
+    if (waiting) {
+        // As main.cpp:293-304 leaves a finished dial phase: waiting, the
+        // check counter at zero, the second damping factor, and the
+        // programmed metric held at this dial factor.
+        st.status = INST_WAITING;
+        st.k_phase = q.steps_per_phase;
+        st.tsc = 0;
+        st.damping = q.damping2;
+        st.cur_dial = dial_factor;
+        st.cur_lam = (1.0 - dial_factor) * 1.0 + dial_factor * q.lam_final;
+        st.cur_pw = std::pow(st.cur_lam, -2.0 * q.nu_ot);
+    } else {
+        st.k_phase = static_cast<long long>(std::fmod(dial_factor, q.spacing) * static_cast<double>(q.steps_per_phase));
+    }
+    b->init_state[i] = st;
+    MB_CUDA(b, cudaMemcpy(b->d_is + i, &st, sizeof(InstState), cudaMemcpyHostToDevice));
+    return MS_OK;
+}
+
 ms_status ms_batch_set_schedule(ms_batch* b, const ms_batch_schedule* s) {
     if (!b || !s) return MS_ERR_INVALID_ARGUMENT;
     if (s->chunk_steps <= 0 || s->chunk_steps % 2 || s->chunk_steps > 1024)

@@ -110,8 +110,13 @@ __device__ __forceinline__ void eq_block_reduce_and_finish(const DevState& s, do
     eq_store_and_fold(s, r, blockIdx.x, gridDim.x, gridDim.x);
 }
 
+#ifndef MSB_NODE_MINB
+#define MSB_NODE_MINB 1
+#endif
+
 template <bool MIXED>
-__global__ void __launch_bounds__(kNodeBlock) k_node_update(const DevMesh m, const DevState s, const StepScalars sc) {
+__global__ void __launch_bounds__(kNodeBlock, MSB_NODE_MINB)
+    k_node_update(const DevMesh m, const DevState s, const StepScalars sc) {
     const int gstep = global_step(s.err, sc.step);
     if (stale(s.err, gstep)) return;  // uniform: only earlier kernels can make it true
     const int n = blockIdx.x * kNodeBlock + threadIdx.x;

@@ -156,7 +156,7 @@ __device__ __forceinline__ void node_finish(const DevMesh& m, const DevState& s,
 
 // Entries whose indices, then contributions, one thread loads together.
 #ifndef MSB_NODE_BATCH
-#define MSB_NODE_BATCH 8
+#define MSB_NODE_BATCH 4
 #endif
 constexpr int kNodeBatch = MSB_NODE_BATCH;
 

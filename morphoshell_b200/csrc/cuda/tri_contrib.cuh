@@ -32,64 +32,30 @@ __device__ __forceinline__ void tri_hmu(const DevMesh& m, int t, double& h, doub
     }
 }
 
-// Contributions of triangle t to its six patch nodes, in the precision of
-// the path (double, or float for the mixed path).  With DIAL_LCE the
-// programmed metric is protocol 3 at (dial, lam = lambda, pw = lambda^(-2 nu_ot))
-// over the director trigonometry in p.tri_aux; otherwise it is read from
-// m.abar / m.bbar.
-template <int DIAL, bool MIXED>
-__device__ __forceinline__ void tri_contrib(const DevMesh& m, const ClusterPlan& p, const double* __restrict__ pos,
-                                            int t, const int (&ids)[6], double dial, double lam, double pw,
-                                            typename Real<MIXED>::T (&f)[18], double nu, double gamma, double h,
-                                            double mu) {
+// Protocol-3 programmed metric (do_dialling.cpp:112-123) from the director
+// trigonometry cos^2, sin^2, cos sin and l2 = lambda^2, pp = lambda^(-2 nu_ot);
+// bbar = 0.
+__device__ __forceinline__ void lce_metric(double c2, double s2, double cs, double l2, double pp,
+                                           TriMat<double>& mt) {
+    mt.abar0 = l2 * c2 + pp * s2;
+    mt.abar1 = (l2 - pp) * cs;
+    mt.abar2 = pp * c2 + l2 * s2;
+    mt.bbar0 = mt.bbar1 = mt.bbar2 = 0.0;
+}
+
+// Contributions of one triangle to its six patch nodes, in the precision of
+// the path (double, or float for the mixed path), from its gathered patch
+// positions P, its 24 derivative weights c (d/dx, d/dy of the 3 vertices;
+// xx, xy, yy weights of the 6 patch nodes) and its material and programmed
+// tensors mt.
+template <bool MIXED>
+__device__ __forceinline__ void tri_forces(const double (&P)[6][3], const typename Real<MIXED>::T (&c)[24],
+                                           const TriMat<double>& mt, double nu, double gamma,
+                                           typename Real<MIXED>::T (&f)[18]) {
     using R = typename Real<MIXED>::T;
-    const int N = m.N;
-    TriMat<double> mt;
-    mt.h = h;
-    mt.mu = mu;
-    if (DIAL == DIAL_LCE) {
-        const double2* ap = reinterpret_cast<const double2*>(p.tri_aux + t);
-        const double2 a01 = __ldg(ap), a23 = __ldg(ap + 1);
-        const double4 aux = {a01.x, a01.y, a23.x, a23.y};
-        mt.area = aux.x;
-        double l2 = lam * lam, pp = pw;
-        if (!p.lce_uniform) {
-            const double2 ln = __ldg(p.lce_ln + t);
-            const double lt = (1.0 - dial) * 1.0 + dial * ln.x;
-            l2 = lt * lt;
-            pp = pow(lt, -2.0 * ln.y);
-        }
-        mt.abar0 = l2 * aux.y + pp * aux.z;
-        mt.abar1 = (l2 - pp) * aux.w;
-        mt.abar2 = pp * aux.y + l2 * aux.z;
-        mt.bbar0 = mt.bbar1 = mt.bbar2 = 0.0;
-    } else {
-        mt.area = __ldg(m.area + t);
-        mt.abar0 = __ldg(m.abar + t);
-        mt.abar1 = __ldg(m.abar + (size_t)m.T + t);
-        mt.abar2 = __ldg(m.abar + 2 * (size_t)m.T + t);
-        mt.bbar0 = __ldg(m.bbar + t);
-        mt.bbar1 = __ldg(m.bbar + (size_t)m.T + t);
-        mt.bbar2 = __ldg(m.bbar + 2 * (size_t)m.T + t);
-    }
-    R c[24];
-    double P[6][3];
-#pragma unroll
-    for (int s = 0; s < 6; ++s) {
-        P[s][0] = __ldg(pos + ids[s]);
-        P[s][1] = __ldg(pos + N + ids[s]);
-        P[s][2] = __ldg(pos + 2 * N + ids[s]);
-    }
     Cq<R> q;
     CqGrad<R> g;
     if constexpr (!MIXED) {
-        const double2* cp = reinterpret_cast<const double2*>(p.coef_aos + 24 * (size_t)t);
-#pragma unroll
-        for (int k = 0; k < 12; ++k) {
-            const double2 v = __ldg(cp + k);
-            c[2 * k] = v.x;
-            c[2 * k + 1] = v.y;
-        }
         double rx[3], ry[3], rxx[3], rxy[3], ryy[3];
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
@@ -120,15 +86,6 @@ __device__ __forceinline__ void tri_contrib(const DevMesh& m, const ClusterPlan&
         // from state to state, while the rounding of the weights only
         // perturbs the reference triangle by a fixed ~1e-7.  The second
         // derivatives and everything after the strain are float.
-        const float4* cp = reinterpret_cast<const float4*>(p.coef_aos_f + 24 * (size_t)t);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const float4 v = __ldg(cp + k);
-            c[4 * k] = v.x;
-            c[4 * k + 1] = v.y;
-            c[4 * k + 2] = v.z;
-            c[4 * k + 3] = v.w;
-        }
         const double dd[6] = {c[0], c[1], c[2], c[3], c[4], c[5]};
         const float* mw = c + 6;
         double Q[6][3];
@@ -185,6 +142,72 @@ __device__ __forceinline__ void tri_contrib(const DevMesh& m, const ClusterPlan&
         f[3 * s + 1] = -fy;
         f[3 * s + 2] = -fz;
     }
+}
+
+
+// Contributions of triangle t read from the per-triangle (AoS) tables.
+// With DIAL_LCE the programmed metric is protocol 3 at (dial, lam = lambda,
+// pw = lambda^(-2 nu_ot)) over the director trigonometry in p.tri_aux;
+// otherwise it is read from m.abar / m.bbar.
+template <int DIAL, bool MIXED>
+__device__ __forceinline__ void tri_contrib(const DevMesh& m, const ClusterPlan& p, const double* __restrict__ pos,
+                                            int t, const int (&ids)[6], double dial, double lam, double pw,
+                                            typename Real<MIXED>::T (&f)[18], double nu, double gamma, double h,
+                                            double mu) {
+    using R = typename Real<MIXED>::T;
+    const int N = m.N;
+    TriMat<double> mt;
+    mt.h = h;
+    mt.mu = mu;
+    if (DIAL == DIAL_LCE) {
+        const double2* ap = reinterpret_cast<const double2*>(p.tri_aux + t);
+        const double2 a01 = __ldg(ap), a23 = __ldg(ap + 1);
+        mt.area = a01.x;
+        double l2 = lam * lam, pp = pw;
+        if (!p.lce_uniform) {
+            const double2 ln = __ldg(p.lce_ln + t);
+            const double lt = (1.0 - dial) * 1.0 + dial * ln.x;
+            l2 = lt * lt;
+            pp = pow(lt, -2.0 * ln.y);
+        }
+        lce_metric(a01.y, a23.x, a23.y, l2, pp, mt);
+    } else {
+        mt.area = __ldg(m.area + t);
+        mt.abar0 = __ldg(m.abar + t);
+        mt.abar1 = __ldg(m.abar + (size_t)m.T + t);
+        mt.abar2 = __ldg(m.abar + 2 * (size_t)m.T + t);
+        mt.bbar0 = __ldg(m.bbar + t);
+        mt.bbar1 = __ldg(m.bbar + (size_t)m.T + t);
+        mt.bbar2 = __ldg(m.bbar + 2 * (size_t)m.T + t);
+    }
+    R c[24];
+    if constexpr (!MIXED) {
+        const double2* cp = reinterpret_cast<const double2*>(p.coef_aos + 24 * (size_t)t);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) {
+            const double2 v = __ldg(cp + k);
+            c[2 * k] = v.x;
+            c[2 * k + 1] = v.y;
+        }
+    } else {
+        const float4* cp = reinterpret_cast<const float4*>(p.coef_aos_f + 24 * (size_t)t);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const float4 v = __ldg(cp + k);
+            c[4 * k] = v.x;
+            c[4 * k + 1] = v.y;
+            c[4 * k + 2] = v.z;
+            c[4 * k + 3] = v.w;
+        }
+    }
+    double P[6][3];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        P[s][0] = __ldg(pos + ids[s]);
+        P[s][1] = __ldg(pos + N + ids[s]);
+        P[s][2] = __ldg(pos + 2 * N + ids[s]);
+    }
+    tri_forces<MIXED>(P, c, mt, nu, gamma, f);
 }
 
 }  // namespace tridev

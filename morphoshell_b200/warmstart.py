@@ -1,0 +1,191 @@
+"""Learned warm start: a coordinate network that predicts a mesh's
+equilibrium shape from its programmed field, used instead of the flat start
+(or move_nodes_to_ansatz_positions, main.cpp:226-230) as the state the
+damped dynamics begin from.
+
+* Fields: director angle = theta + sum_{k<=4} a_k sin(k theta + phi_k),
+  a_k ~ N(0, 0.2^2), phi_k ~ U(0, 2 pi), lambda_final ~ U(0.8, 1.2),
+  nu_ot = 0.5 (dialling protocol 3, do_dialling.cpp:112-123).
+* Training data: equilibria at dial factor 1 that the plain method itself
+  reaches (the batched engine, ms_batch_*), one row per node: the node's
+  features -> its displacement from the flat reference position.  A shape
+  and its mirror image z -> -z are both equilibria of an in-plane metric
+  with b-bar = 0, so targets are mirrored to a common orientation (mean
+  displacement z >= 0).
+* Network: ms_mlp_* (tensor-core BF16 SiLU MLP, FP32 accumulation, Adam).
+* Warm start: predicted positions uploaded into a batch instance that waits
+  for equilibrium at dial factor 1 (ms_batch_set_start).  The plain damped
+  dynamics always run from there to full equilibrium and judge the start;
+  a prediction that is not finite or whose elastic energy at dial factor 1
+  exceeds the flat start's falls back to the plain start.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import MS_INST_DONE, MS_INST_FAILED, MS_PRECISION_FP64, Batch, GpuLoop, Mlp
+
+N_FEATURES = 23
+
+
+@dataclass
+class Field:
+    a: np.ndarray      # (4,)
+    phi: np.ndarray    # (4,)
+    lam: float
+
+    def angle(self, theta):
+        k = np.arange(1, 5)
+        return theta + (self.a[None, :] * np.sin(k[None, :] * np.asarray(theta)[:, None] + self.phi[None, :])).sum(1)
+
+
+def random_field(rng) -> Field:
+    return Field(a=rng.normal(0.0, 0.2, 4), phi=rng.uniform(0.0, 2.0 * math.pi, 4), lam=float(rng.uniform(0.8, 1.2)))
+
+
+def fields(n: int, seed: int):
+    rng = np.random.default_rng(seed)
+    return [random_field(rng) for _ in range(n)]
+
+
+def abar_info(model_tris_centroids: np.ndarray, f: Field) -> np.ndarray:
+    """(T, 3) protocol-3 columns (angle, lambda_final, nu_ot) at triangle centroids."""
+    c = model_tris_centroids
+    theta = np.arctan2(c[:, 1], c[:, 0])
+    ang = f.angle(theta)
+    return np.ascontiguousarray(np.column_stack([ang, np.full_like(ang, f.lam), np.full_like(ang, 0.5)]))
+
+
+def node_features(xy: np.ndarray, f: Field) -> np.ndarray:
+    """Per-node inputs: x, y, r, the programmed metric at dial factor 1 at the
+    node (3 components), lambda_final, sin/cos k theta (k = 1..4), and the
+    field's coefficients a_k cos phi_k, a_k sin phi_k (k = 1..4)."""
+    x, y = xy[:, 0], xy[:, 1]
+    theta = np.arctan2(y, x)
+    ang = f.angle(theta)
+    c, s = np.cos(ang), np.sin(ang)
+    lam2, p = f.lam ** 2, f.lam ** (-1.0)
+    a0 = lam2 * c * c + p * s * s
+    a1 = (lam2 - p) * c * s
+    a2 = p * c * c + lam2 * s * s
+    cols = [x, y, np.hypot(x, y), a0, a1, a2, np.full_like(x, f.lam)]
+    for k in range(1, 5):
+        cols += [np.sin(k * theta), np.cos(k * theta)]
+    for k in range(4):
+        cols += [np.full_like(x, f.a[k] * math.cos(f.phi[k])), np.full_like(x, f.a[k] * math.sin(f.phi[k]))]
+    return np.column_stack(cols).astype(np.float32)
+
+
+def centroids(model) -> np.ndarray:
+    from . import lib
+    import ctypes as C
+    T = model.num_tris
+    tv = np.empty((T, 3), dtype=np.int32)
+    lib().msh_get_tri_vertices(model._h, tv.ctypes.data_as(C.POINTER(C.c_int32)))
+    ref = model.dofs(0).reshape(3, -1).T
+    return ref[tv].mean(1)
+
+
+def solve(model, flds, precision=MS_PRECISION_FP64, starts=None, max_steps=2_000_000, autotune=True):
+    """Runs every field to its first equilibrium at dial factor 1 in one
+    batch.  starts[i] (3N SoA positions or None) makes instance i a warm
+    start waiting at dial factor 1.  Returns (final positions per field,
+    steps per field, statuses, wall seconds of the batch run)."""
+    cen = centroids(model)
+    infos = [abar_info(cen, f) for f in flds]
+    b = Batch([model] * len(flds), precision=precision, abar_infos=infos)
+    if starts is not None:
+        for i, x in enumerate(starts):
+            if x is not None:
+                b.upload(i, x)
+                b.set_start(i, 1.0, True)
+    if autotune:
+        b.autotune(steps_per_trial=8)
+    t0 = time.time()
+    b.run(max_steps)
+    wall = time.time() - t0
+    out, steps, stat = [], [], []
+    for i in range(len(flds)):
+        st = b.status(i)
+        out.append(b.download(i)[0])
+        steps.append(st.stepcount)
+        stat.append(st.status)
+    b.close()
+    return out, np.array(steps), np.array(stat), wall
+
+
+def canonical(disp: np.ndarray) -> np.ndarray:
+    """(N, 3) displacement mirrored so that its mean z is >= 0."""
+    d = disp.copy()
+    if d[:, 2].mean() < 0:
+        d[:, 2] = -d[:, 2]
+    return d
+
+
+def dataset(model, flds, finals):
+    ref = model.dofs(0).reshape(3, -1).T
+    xy = ref[:, :2]
+    X, Y = [], []
+    for f, x in zip(flds, finals):
+        X.append(node_features(xy, f))
+        Y.append(canonical(x.reshape(3, -1).T - ref).astype(np.float32))
+    return np.concatenate(X), np.concatenate(Y)
+
+
+def predict_positions(net: Mlp, model, f: Field) -> np.ndarray:
+    ref = model.dofs(0).reshape(3, -1).T
+    d = net.forward(node_features(ref[:, :2], f))
+    return np.ascontiguousarray((ref + d).T.ravel())
+
+
+def elastic_energy(model, f: Field, x: np.ndarray) -> float:
+    """Stretch + bend energy at dial factor 1 (calc_energies.cpp:44-63)."""
+    g = GpuLoop(model)
+    info = abar_info(centroids(model), f)
+    _, b_info = model.programmed()
+    g.set_programmed(3, info, b_info, model.scalars.dial_factors_to_hold_at_spacing)
+    g.upload(x)
+    g.do_dialling(1.0)
+    e = g.output_quantities()["energies"]
+    g.close()
+    return float(e[0] + e[1])
+
+
+def warm_starts(net: Mlp, model, flds):
+    """Predicted start per field, or None (plain start) when the prediction
+    is not finite or has more elastic energy than the flat start."""
+    flat = model.dofs(1)
+    out, fell_back = [], 0
+    for f in flds:
+        x = predict_positions(net, model, f)
+        ok = np.all(np.isfinite(x)) and elastic_energy(model, f, x) <= elastic_energy(model, f, flat)
+        out.append(x if ok else None)
+        fell_back += 0 if ok else 1
+    return out, fell_back
+
+
+def evaluate(net: Mlp, model, flds, precision=MS_PRECISION_FP64, max_steps=2_000_000):
+    """Time to the first equilibrium at dial factor 1 from the plain start
+    and from the learned start, and the distance between the two shapes."""
+    plain, s_plain, st_plain, w_plain = solve(model, flds, precision, None, max_steps)
+    starts, fell_back = warm_starts(net, model, flds)
+    learned, s_learn, st_learn, w_learn = solve(model, flds, precision, starts, max_steps)
+    dist = []
+    for a, b in zip(plain, learned):
+        da, db = a.reshape(3, -1), b.reshape(3, -1)
+        mirrored = db.copy()
+        mirrored[2] = -mirrored[2]
+        dist.append(min(np.abs(da - db).max(), np.abs(da - mirrored).max()))
+    return {
+        "fields": len(flds), "fell_back": fell_back,
+        "plain_steps_mean": float(s_plain.mean()), "learned_steps_mean": float(s_learn.mean()),
+        "step_speedup": float(s_plain.mean() / max(s_learn.mean(), 1.0)),
+        "plain_wall_s": w_plain, "learned_wall_s": w_learn, "wall_speedup": w_plain / max(w_learn, 1e-9),
+        "plain_done": int((st_plain == MS_INST_DONE).sum()), "learned_done": int((st_learn == MS_INST_DONE).sum()),
+        "failed": int((st_plain == MS_INST_FAILED).sum() + (st_learn == MS_INST_FAILED).sum()),
+        "shape_distance_max": float(np.max(dist)), "shape_distance_median": float(np.median(dist)),
+    }
