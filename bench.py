@@ -245,7 +245,7 @@ def run_ours(args):
     T = model.num_tris
     prec = MS_PRECISION_MIXED if args.precision == "mixed" else MS_PRECISION_FP64
     g = GpuLoop(model, precision=prec, device=local)
-    g.set_step_path(0 if args.path == "cluster" else 1)
+    g.set_step_path({"cluster": 0, "two-kernel": 1, "tiles": 2}[args.path])
     plan = g.plan_info()
     g.set_programmed(3, info, bbar, s.dial_factors_to_hold_at_spacing)
     g.upload(model.dofs(1))
@@ -314,6 +314,8 @@ def run_ours(args):
     e2e_value = T * e2e_steps * world / (float(t2.item()) / 1e3)
 
     clocks = clk.summary()
+    tri_name, node_name = {"cluster": ("k_cluster_step", "k_halo_update"), "two-kernel": ("k_tri_aos", "k_node_update"),
+                           "tiles": ("k_tri_tiles", "k_node_update")}[args.path]
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -322,11 +324,9 @@ def run_ours(args):
         "gpu_launches": 2 * args.steps + (args.steps + 127) // 128,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": ("one step = k_cluster_step + k_halo_update" if args.path == "cluster"
-                                else "one step = k_tri_aos + k_node_update"),
+                     "kernel": "one step = %s + %s" % (tri_name, node_name),
                      "algorithmic_bytes_per_tri": bpt,
-                     "kernel_ms": ({"k_cluster_step": t_tri, "k_halo_update": t_node} if args.path == "cluster"
-                                   else {"k_tri_aos": t_tri, "k_node_update": t_node})},
+                     "kernel_ms": {tri_name: t_tri, node_name: t_node}},
         "plan": plan,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 2 * 24 * N + 8,
                 "d2h_bytes_per_step": 2 * 24 * N + 16, "steps": e2e_steps},
@@ -437,7 +437,7 @@ def main():
     ap.add_argument("--workload", default="disk1p8m")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
-    ap.add_argument("--path", choices=["cluster", "two-kernel"], default="two-kernel",
+    ap.add_argument("--path", choices=["cluster", "two-kernel", "tiles"], default="tiles",
                     help="fused-step implementation (ms_set_step_path)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -203,10 +203,12 @@ void* ms_stream(ms_handle* h);
 /* Which implementation ms_step_n uses: 0 the cluster-tiled step -- each
  * thread-block cluster owns a Morton tile of triangles, keeps their force
  * contributions in distributed shared memory and updates the tile's
- * interior nodes itself; 1 (default) the two-kernel step (per-triangle
- * kernel writes all contributions to HBM, per-node kernel gathers them).
- * Both sum every node's contributions in ascending triangle order, so they
- * give the same bits. */
+ * interior nodes itself; 1 the two-kernel step (per-triangle kernel writes
+ * all contributions to HBM, per-node kernel gathers them); 2 (default) the
+ * two-kernel step whose per-triangle kernel is persistent and streams its
+ * tables through shared memory with bulk asynchronous copies.  All sum
+ * every node's contributions in ascending triangle order, so they give the
+ * same bits. */
 ms_status ms_set_step_path(ms_handle* h, int path);
 /* Tiling of the cluster path: CTAs per cluster, triangles per CTA, number of
  * clusters, number of halo nodes (summed by the second kernel), and the

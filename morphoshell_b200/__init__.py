@@ -431,7 +431,8 @@ class GpuLoop:
         return rep
 
     def set_step_path(self, path: int):
-        """0: cluster-tiled step (default), 1: two-kernel step."""
+        """0: cluster-tiled step, 1: two-kernel step, 2 (default): two-kernel
+        step with the per-triangle tables fed by bulk asynchronous copies."""
         self._chk(lib().ms_set_step_path(self._h, path), "set_step_path")
 
     def plan_info(self) -> dict:

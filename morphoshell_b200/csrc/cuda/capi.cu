@@ -71,10 +71,14 @@ struct ms_handle {
     ClusterPlan plan{};
     bool have_plan = false;
     bool have_cluster = false;
-    int step_path = 1;  // 0 cluster-tiled, 1 two-kernel (default: measured faster)
+    int step_path = 1;  // 0 cluster-tiled, 1 two-kernel, 2 two-kernel with bulk-copied tiles (default when built)
     std::vector<double> area_host;
     double lce_lam_final = 0, lce_nu = 0;
     int halo_parts = 0;
+    // bulk-copy-fed per-triangle kernel
+    bool have_tiles = false;
+    unsigned char* d_tiles = nullptr;
+    size_t tile_bytes = 0;
 };
 
 namespace {
@@ -164,6 +168,57 @@ template <typename T>
 ms_status upload(ms_handle* h, T** dst, const std::vector<T>& src) {
     MS_TRY(dalloc(h, dst, src.size()));
     if (!src.empty()) MS_CUDA(h, cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return MS_OK;
+}
+
+// Tile records of the bulk-copy-fed per-triangle kernel (ClusterPlan::tiles):
+// ids and weights now, area in the trigonometry block (cos^2 = 1, the rest
+// 0) until prepare_lce_tables writes the director's values.
+ms_status build_tiles(ms_handle* h, const ms_mesh_desc* d) {
+    const int T = d->num_tris;
+    const int mixed = h->precision == MS_PRECISION_MIXED;
+    int blocks = 0;
+    if (prepare_tile_kernels(mixed, &blocks) != cudaSuccess || blocks <= 0) {
+        cudaGetLastError();
+        h->have_tiles = false;
+        return MS_OK;  // the other paths remain
+    }
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t rec = tile_record_bytes(mixed);
+    const int ntiles = (T + kTile - 1) / kTile;
+    std::vector<unsigned char> buf(rec * ntiles, 0);
+    const size_t ids_b = 6 * kTile * 4, coef_b = 24 * kTile * (mixed ? 4 : 8);
+    for (int tile = 0; tile < ntiles; ++tile) {
+        unsigned char* r = buf.data() + rec * tile;
+        int32_t* ids = reinterpret_cast<int32_t*>(r);
+        double* aux = reinterpret_cast<double*>(r + ids_b + coef_b);
+        for (int i = 0; i < kTile; ++i) {
+            const int t = tile * kTile + i;
+            if (t >= T) break;
+            for (int k = 0; k < 6; ++k) ids[k * kTile + i] = d->patch_ids[6LL * t + k];
+            const double* w = d->deriv_coeffs + 24LL * t;
+            if (mixed) {
+                float* c = reinterpret_cast<float*>(r + ids_b);
+                for (int k = 0; k < 24; ++k) c[k * kTile + i] = (float)w[k];
+            } else {
+                double* c = reinterpret_cast<double*>(r + ids_b);
+                for (int k = 0; k < 24; ++k) c[k * kTile + i] = w[k];
+            }
+            aux[i] = d->ref_area[t];
+            aux[kTile + i] = 1.0;
+        }
+    }
+    unsigned char* dt;
+    MS_TRY(upload(h, &dt, buf));
+    h->d_tiles = dt;
+    h->tile_bytes = rec;
+    if (mixed) h->plan.tiles_f = dt;
+    else h->plan.tiles = dt;
+    h->plan.tile_grid = sms * blocks;
+    h->have_tiles = true;
+    h->step_path = 2;  // measured fastest on B200 (same bits as path 1)
     return MS_OK;
 }
 
@@ -258,7 +313,7 @@ ms_status build_cluster_plan(ms_handle* h, const ms_mesh_desc* d, const std::vec
         h->s.eq_blocks = parts;
     }
     h->have_plan = true;
-    return MS_OK;
+    return build_tiles(h, d);
 }
 
 // Per-triangle director trigonometry for the cluster kernel's protocol-3
@@ -287,6 +342,18 @@ ms_status prepare_lce_tables(ms_handle* h, const double* info, int ka) {
     MS_CUDA(h, cudaMemcpy(d_ln, ln.data(), ln.size() * sizeof(double), cudaMemcpyHostToDevice));
     h->plan.tri_aux = d_aux;
     h->plan.lce_ln = d_ln;
+    if (h->have_tiles) {
+        // The trigonometry block of every tile record: [4][kTile] doubles.
+        const int ntiles = (T + kTile - 1) / kTile;
+        std::vector<double> blk(4ULL * kTile * ntiles, 0.0);
+        for (int t = 0; t < T; ++t) {
+            const int tile = t / kTile, i = t % kTile;
+            for (int k = 0; k < 4; ++k) blk[(size_t)tile * 4 * kTile + k * kTile + i] = aux[4ULL * t + k];
+        }
+        const size_t off = 6 * kTile * 4 + 24 * kTile * (h->precision == MS_PRECISION_MIXED ? 4 : 8);
+        MS_CUDA(h, cudaMemcpy2D(h->d_tiles + off, h->tile_bytes, blk.data(), 4 * kTile * sizeof(double),
+                                4 * kTile * sizeof(double), ntiles, cudaMemcpyHostToDevice));
+    }
     h->plan.lce_uniform = uniform ? 1 : 0;
     h->lce_lam_final = ln[0];
     h->lce_nu = ln[1];
@@ -728,15 +795,19 @@ static cudaError_t launch_step(ms_handle* h, const StepScalars& sc, bool cluster
         e = launch_cluster_step(h->m, h->plan, h->s, sc, dial_mode, h->precision, st);
         if (e == cudaSuccess) e = launch_halo_update(h->m, h->plan, h->s, sc, h->precision, st);
     } else {
-        e = launch_tri_aos(h->m, h->plan, h->s, sc, dial_mode, h->precision, st);
+        if (h->step_path == 2 && h->have_tiles)
+            e = launch_tri_tiles(h->m, h->plan, h->s, sc, dial_mode, h->precision, st);
+        else
+            e = launch_tri_aos(h->m, h->plan, h->s, sc, dial_mode, h->precision, st);
         if (e == cudaSuccess) e = launch_node_update(h->m, h->s, sc, h->precision, st);
     }
     return e;
 }
 
 ms_status ms_set_step_path(ms_handle* h, int path) {
-    if (!h || path < 0 || path > 1) return MS_ERR_INVALID_ARGUMENT;
+    if (!h || path < 0 || path > 2) return MS_ERR_INVALID_ARGUMENT;
     if (path == 0 && !h->have_cluster) return fail(h, MS_ERR_UNSUPPORTED, "cluster launches are unavailable");
+    if (path == 2 && !h->have_tiles) return fail(h, MS_ERR_UNSUPPORTED, "bulk-copy tile kernel unavailable");
     h->step_path = path;
     return MS_OK;
 }
@@ -763,7 +834,8 @@ ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, doub
     while (done < n) {
         const int len = std::min(kChunk, n - done);
         const bool last_chunk = done + len == n;
-        GraphKey key{len, p0 ^ (done & 1), dial_mode + (cluster ? 16 : 0), gd, (check_last && last_chunk) ? 1 : 0,
+        GraphKey key{len, p0 ^ (done & 1), dial_mode + (cluster ? 16 : 0) + (h->step_path == 2 ? 32 : 0), gd,
+                     (check_last && last_chunk) ? 1 : 0,
                      dt, damping};
         cudaGraphExec_t exec = nullptr;
         if (!(dialling && !fuse_lce))
@@ -877,6 +949,8 @@ ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial, dou
         const int mode = fuse_lce ? DIAL_LCE : DIAL_ARRAYS;
         MS_CUDA(h, cudaEventRecord(ev[3 * i], st));
         if (cluster) MS_CUDA(h, launch_cluster_step(h->m, h->plan, h->s, sc, mode, h->precision, st));
+        else if (h->step_path == 2 && h->have_tiles)
+            MS_CUDA(h, launch_tri_tiles(h->m, h->plan, h->s, sc, mode, h->precision, st));
         else MS_CUDA(h, launch_tri_aos(h->m, h->plan, h->s, sc, mode, h->precision, st));
         MS_CUDA(h, cudaEventRecord(ev[3 * i + 1], st));
         if (cluster) MS_CUDA(h, launch_halo_update(h->m, h->plan, h->s, sc, h->precision, st));

@@ -114,7 +114,17 @@ struct ClusterPlan {
     const unsigned short* own_ent;  // (rank << 13) | (index in CTA << 3) | slot, ascending triangle
     const int* halo_nodes;     // nodes summed by the halo kernel
     int n_halo;
+    // Tile records of the bulk-copy-fed per-triangle kernel (tri_tiles.cu):
+    // per kTile triangles, ids [6][kTile] int32, weights [24][kTile]
+    // (double; float in tiles_f), area and director trigonometry
+    // [4][kTile] double.
+    const void* tiles;
+    const void* tiles_f;
+    int tile_grid;             // persistent blocks (SMs x resident blocks)
 };
+
+// Triangles per tile of the bulk-copy-fed per-triangle kernel.
+constexpr int kTile = 128;
 
 // ---- batched ensembles (batch.cu) ----------------------------------------------
 // Many meshes stepped together: their tables are concatenated into one union
@@ -215,6 +225,13 @@ cudaError_t launch_halo_update(const DevMesh& m, const ClusterPlan& p, const Dev
 // with mixed, contributions go to DevMesh::contrib_f as float.
 cudaError_t launch_tri_aos(const DevMesh& m, const ClusterPlan& p, const DevState& s, const StepScalars& sc,
                            int dial_mode, int mixed, cudaStream_t st);
+// Bulk-copy-fed per-triangle kernel (tri_tiles.cu): bytes of one tile
+// record, kernel set-up (dynamic shared memory; resident blocks per SM) and
+// launch.
+size_t tile_record_bytes(int mixed);
+cudaError_t prepare_tile_kernels(int mixed, int* blocks_per_sm);
+cudaError_t launch_tri_tiles(const DevMesh& m, const ClusterPlan& p, const DevState& s, const StepScalars& sc,
+                             int dial_mode, int mixed, cudaStream_t st);
 // Largest cluster size (8, 4, 2, 1) whose clusters fill the most SMs, and the
 // CTA shape used with it.
 int choose_cluster_size(int tpc, int threads, int mixed);

@@ -228,6 +228,13 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
         if (!mbar_wait_bounded(&bar[s], phase[s])) failed = 1;
     }
     __syncthreads();
+    if (failed && threadIdx.x == 0) {
+        // Give MMAs still in flight a bounded chance to finish before the
+        // tensor memory is freed.
+        mbar_wait_bounded(&bar[0], phase[0]);
+        mbar_wait_bounded(&bar[1], phase[1]);
+    }
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (failed) {
         if (threadIdx.x == 0) atomicExch(g.err, 1);

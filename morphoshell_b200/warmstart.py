@@ -189,3 +189,86 @@ def evaluate(net: Mlp, model, flds, precision=MS_PRECISION_FP64, max_steps=2_000
         "failed": int((st_plain == MS_INST_FAILED).sum() + (st_learn == MS_INST_FAILED).sum()),
         "shape_distance_max": float(np.max(dist)), "shape_distance_median": float(np.median(dist)),
     }
+
+
+def network_flops_per_row(in_dim: int, width: int, hidden: int, out_dim: int = 3) -> float:
+    """Multiply-adds x 2 of one forward pass per row (padded widths)."""
+    in_pad = (in_dim + 15) // 16 * 16
+    macs = in_pad * width + (hidden - 1) * width * width + width * 16
+    return 2.0 * macs
+
+
+def main(argv=None):
+    """The warm-start experiment: plain-method equilibria of random fields
+    train the network; on held-out fields, time to the first equilibrium at
+    dial factor 1 from the plain start and from the learned start."""
+    import argparse
+    import json
+    import os
+    import tempfile
+
+    from . import MS_PRECISION_MIXED, Model, meshgen
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--mesh", default="disk18k")
+    ap.add_argument("--train", type=int, default=4096)
+    ap.add_argument("--held-out", type=int, default=256)
+    ap.add_argument("--chunk", type=int, default=1024, help="fields per batch while generating data")
+    ap.add_argument("--epochs", type=int, default=200)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--width", type=int, default=256)
+    ap.add_argument("--hidden", type=int, default=4)
+    ap.add_argument("--spacing", type=float, default=0.25, help="dial_factors_to_hold_at_spacing")
+    ap.add_argument("--phase-prefactor", type=float, default=0.02, help="dial_phase_time_prefactor")
+    ap.add_argument("--force-thr", type=float, default=1e-6)
+    ap.add_argument("--speed-thr", type=float, default=1e-5)
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--max-steps", type=int, default=3_000_000)
+    ap.add_argument("--out", default="warmstart.json")
+    a = ap.parse_args(argv)
+    prec = MS_PRECISION_MIXED if a.precision == "mixed" else MS_PRECISION_FP64
+    d = tempfile.mkdtemp(prefix="ms_ws_")
+    st, vtk = meshgen.write_workload(d, a.mesh, dial_factors_to_hold_at_spacing=a.spacing,
+                                     dial_phase_time_prefactor=a.phase_prefactor,
+                                     force_to_char_force_ratio_equil_threshold=a.force_thr,
+                                     speed_to_char_speed_ratio_equil_threshold=a.speed_thr)
+    model = Model(st, vtk, quiet=True)
+    report = {"mesh": a.mesh, "num_tris": model.num_tris, "num_nodes": model.num_nodes, "settings": vars(a)}
+    train_f = fields(a.train, seed=100)
+    held_f = fields(a.held_out, seed=200)
+
+    t0 = time.time()
+    finals, steps, kept = [], [], []
+    report["train_not_done"] = 0
+    for c0 in range(0, len(train_f), a.chunk):
+        part = train_f[c0:c0 + a.chunk]
+        fx, sx, stx, _ = solve(model, part, prec, None, a.max_steps)
+        for f, x, n_steps, status in zip(part, fx, sx, stx):
+            if status == MS_INST_DONE:
+                kept.append(f)
+                finals.append(x)
+                steps.append(n_steps)
+            else:
+                report["train_not_done"] += 1
+    report["datagen_s"] = time.time() - t0
+    report["train_steps_mean"] = float(np.mean(steps))
+    X, Y = dataset(model, kept, finals)
+    net = Mlp(N_FEATURES, width=a.width, hidden_layers=a.hidden, out_dim=3, seed=7)
+    net.set_data(X, Y)
+    t0 = time.time()
+    losses = net.train(a.epochs, batch=a.batch, lr=a.lr, seed=1)
+    train_s = time.time() - t0
+    flops = 3.0 * network_flops_per_row(N_FEATURES, a.width, a.hidden) * X.shape[0] * a.epochs
+    report.update({"rows": int(X.shape[0]), "train_s": train_s, "train_tflops": flops / train_s / 1e12,
+                   "loss_first": float(losses[0]), "loss_last": float(losses[-1])})
+    report["eval"] = evaluate(net, model, held_f, prec, a.max_steps)
+    with open(a.out, "w") as f:
+        json.dump(report, f, indent=1)
+    print(json.dumps(report))
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())

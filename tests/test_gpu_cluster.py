@@ -41,6 +41,7 @@ def test_cluster_equals_two_kernel_bitwise_when_waiting(workdir, name):
     assert np.array_equal(x0, x1) and np.array_equal(v0, v1)
     info = g0.plan_info()
     assert info["path"] == 0 and info["cluster_size"] >= 1
+    assert g1.plan_info()["path"] == 1
 
 
 def test_cluster_dialling_matches_two_kernel(workdir):
@@ -135,3 +136,23 @@ def test_mixed_precision_equilibrium_shape(workdir):
         assert r.final_dial_factor == 1.0 and r.equilibria_reached >= 2, (r.final_dial_factor, r.equilibria_reached)
         shapes.append(x)
     assert np.abs(shapes[1] - shapes[0]).max() < 1e-5
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_tile_path_equals_two_kernel_bitwise(workdir, precision):
+    """The bulk-copy-fed per-triangle kernel (path 2) reads the same tables
+    from shared memory and runs the same arithmetic: identical bits, in
+    dialling and in waiting steps, for both precisions."""
+    m = make_model(workdir, "disk18k")
+    s = m.scalars
+    x, v = deformed_state(m, seed=25, amp=0.02)
+    g1, g2 = _loops(m, [1, 2], precision=precision)
+    dials = 0.2 + 1e-5 * np.arange(300)
+    for g in (g1, g2):
+        g.upload(x, v)
+        g.step_n(300, dials, s.timestep, s.damping_factor_1)
+        g.step_n(200, None, s.timestep, s.damping_factor_2)
+    x1, v1 = g1.download()
+    x2, v2 = g2.download()
+    assert np.array_equal(x1, x2) and np.array_equal(v1, v2)
+    assert g2.plan_info()["path"] == 2
