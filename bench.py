@@ -171,10 +171,24 @@ def cpu_baseline(model, info, bbar, budget_s: float = 20.0):
     o.step_n(n, dials[1:1 + n], s.timestep, s.damping_factor_1)
     el = time.perf_counter() - t0
     o.close()
+    # One thread, a few steps (the reference's serial speed, for scale).
+    o1 = oracle.Oracle(kind, model, threads=1)
+    o1.set_programmed(3, info, bbar, s.dial_factors_to_hold_at_spacing)
+    o1.upload(model.dofs(1))
+    t0 = time.perf_counter()
+    o1.step_n(1, dials[:1], s.timestep, s.damping_factor_1)
+    one1 = time.perf_counter() - t0
+    n1 = int(max(1, min(20, 0.25 * budget_s / max(one1, 1e-6))))
+    t0 = time.perf_counter()
+    o1.step_n(n1, dials[1:1 + n1], s.timestep, s.damping_factor_1)
+    el1 = time.perf_counter() - t0
+    o1.close()
     return {"value": model.num_tris * n / el, "unit": METRIC, "cores": cores,
             "kind": "reference" if kind == "ref" else "port",
             "sample": "%d steps of the full %d-triangle mesh (protocol-3 dialling) after 1 warm-up step, %d threads"
-                      % (n, model.num_tris, cores)}
+                      % (n, model.num_tris, cores),
+            "single_thread_value": model.num_tris * n1 / el1,
+            "single_thread_sample": "%d steps, 1 thread" % n1}
 
 
 def run_reference(args):

@@ -113,13 +113,21 @@ __device__ __forceinline__ void eq_block_reduce_and_finish(const DevState& s, do
 #ifndef MSB_NODE_MINB
 #define MSB_NODE_MINB 1
 #endif
+#ifndef MSB_NODE_REVERSE
+#define MSB_NODE_REVERSE 1
+#endif
 
 template <bool MIXED>
 __global__ void __launch_bounds__(kNodeBlock, MSB_NODE_MINB)
     k_node_update(const DevMesh m, const DevState s, const StepScalars sc) {
     const int gstep = global_step(s.err, sc.step);
     if (stale(s.err, gstep)) return;  // uniform: only earlier kernels can make it true
-    const int n = blockIdx.x * kNodeBlock + threadIdx.x;
+    // Blocks take the nodes from the top down: the per-triangle kernel wrote
+    // the contributions of the last (Morton-ordered) triangles last, so
+    // those are still in L2 when the highest nodes start; and the lowest
+    // nodes, updated last, are the first the next step's triangles read.
+    const int nb = MSB_NODE_REVERSE ? (int)(gridDim.x - 1 - blockIdx.x) : (int)blockIdx.x;
+    const int n = nb * kNodeBlock + threadIdx.x;
     const int N = m.N;
     double fmax = -1.0, vmax = -1.0;
     int fnode = INT_MAX, vnode = INT_MAX;

@@ -6,8 +6,12 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
+#include <exception>
 #include <iterator>
 #include <random>
+#include <thread>
+#include <vector>
 
 #include "host.hpp"
 #include "small_linalg.hpp"
@@ -193,6 +197,43 @@ void calc_mesh_info(std::vector<Node>& nodes, const DMat& P, std::vector<Tri>& t
             tri.ref_centroid[k] = (P(tri.vertex_ids[0], k) + P(tri.vertex_ids[1], k) + P(tri.vertex_ids[2], k)) / 3.0;
 }
 
+namespace {
+
+// Threads for the per-triangle set-up loops: MORPHOSHELL_SETUP_THREADS, else
+// the hardware's; one for small meshes.
+int setup_threads(int n) {
+    if (n < 4096) return 1;
+    int t = (int)std::thread::hardware_concurrency();
+    if (const char* e = std::getenv("MORPHOSHELL_SETUP_THREADS")) t = std::atoi(e);
+    return std::max(1, std::min(t, 128));
+}
+
+// f(begin, end, worker) over [0, n) in contiguous ranges, one per thread.
+// The first exception (of the lowest range) is rethrown after all joined.
+template <typename F>
+void parallel_ranges(int n, int threads, F f) {
+    if (threads <= 1) {
+        f(0, n, 0);
+        return;
+    }
+    std::vector<std::thread> pool;
+    std::vector<std::exception_ptr> errs(threads);
+    const int chunk = (n + threads - 1) / threads;
+    for (int w = 0; w < threads; ++w)
+        pool.emplace_back([&, w]() {
+            try {
+                f(std::min(n, w * chunk), std::min(n, (w + 1) * chunk), w);
+            } catch (...) {
+                errs[w] = std::current_exception();
+            }
+        });
+    for (auto& t : pool) t.join();
+    for (auto& e : errs)
+        if (e) std::rethrow_exception(e);
+}
+
+}  // namespace
+
 // source_files/set_up_patch_fitting.cpp:48-305.  For each triangle, the
 // three extra patch nodes are the nearest candidates (vertices of triangles
 // incident on its vertices, nearest first) whose 6x6 quadratic-fit matrix is
@@ -200,8 +241,14 @@ void calc_mesh_info(std::vector<Node>& nodes, const DMat& P, std::vector<Tri>& t
 // nodes' values to the second derivatives (xx, xy, yy) at the centroid.
 void set_up_patch_fitting(const std::vector<Node>& nodes, const DMat& P, std::vector<Tri>& triangles,
                           const Stuff& stuff, Log& log) {
-    int num_interior_retries = 0;
-    for (auto& tri : triangles) {
+    // Triangles are independent: ranges of them in parallel threads, each
+    // with its own retry count (the same choices as a serial loop).
+    const int nt = setup_threads((int)triangles.size());
+    std::vector<int> retries(nt, 0);
+    parallel_ranges((int)triangles.size(), nt, [&](int t_begin, int t_end, int worker) {
+    int& num_interior_retries = retries[worker];
+    for (int t_index = t_begin; t_index < t_end; ++t_index) {
+        Tri& tri = triangles[t_index];
         std::vector<double> dists;
         std::vector<int> cands;
         for (int v = 0; v < 3; ++v)
@@ -280,6 +327,9 @@ void set_up_patch_fitting(const std::vector<Node>& nodes, const DMat& P, std::ve
                 "issues, either the patch node search will need to be extended, or you will need to use a nicer "
                 "mesh. Aborting.");
     }
+    });
+    int num_interior_retries = 0;
+    for (int r : retries) num_interior_retries += r;
     log << "\nNumber of non-boundary triangles that had to search through \n"
         << "multiple possible patch options to find one \nsatisfying the condition number "
         << "criterion was " << num_interior_retries << ", \nwhich should not be a large proportion of the mesh's "
@@ -293,7 +343,9 @@ void set_up_patch_fitting(const std::vector<Node>& nodes, const DMat& P, std::ve
 void calc_deriv_coeffs(std::vector<double>& coeffs, const DMat& P, const std::vector<Tri>& triangles,
                        const Stuff& stuff) {
     coeffs.assign(static_cast<size_t>(stuff.num_tris) * 24, 0.0);
-    for (const auto& tri : triangles) {
+    parallel_ranges((int)triangles.size(), setup_threads((int)triangles.size()), [&](int b, int e, int) {
+    for (int t_index = b; t_index < e; ++t_index) {
+        const Tri& tri = triangles[t_index];
         double a[3][3], inv[3][3];
         for (int v = 0; v < 3; ++v) {
             a[v][0] = 1.0;
@@ -309,6 +361,7 @@ void calc_deriv_coeffs(std::vector<double>& coeffs, const DMat& P, const std::ve
         for (int n = 0; n < 6; ++n)
             for (int k = 0; k < 3; ++k) c[6 + 3 * n + k] = tri.mat_for_patch_2nd_derivs[n][k];
     }
+    });
 }
 
 // source_files/calc_dof_masses.cpp:45-58: a third of each triangle's mass to

@@ -136,6 +136,37 @@ def dataset(model, flds, finals):
     return np.concatenate(X), np.concatenate(Y)
 
 
+def train_network(net: Mlp, model, flds, finals, epochs: int, batch: int = 8192, lr: float = 1e-3,
+                  rounds: int = 3, seed: int = 1):
+    """Trains on the equilibria of ``flds``.  Each equilibrium counts up to
+    its mirror image: the first round uses the orientation with mean z >= 0,
+    later rounds the orientation closer to the network's current prediction
+    (so near-symmetric shapes, whose mean z is ~0, get a consistent
+    orientation).  Returns the per-epoch losses."""
+    ref = model.dofs(0).reshape(3, -1).T
+    xy = ref[:, :2]
+    N = ref.shape[0]
+    X = np.concatenate([node_features(xy, f) for f in flds])
+    disp = [x.reshape(3, -1).T - ref for x in finals]
+    Y = np.concatenate([canonical(d) for d in disp]).astype(np.float32)
+    losses = []
+    per_round = max(1, epochs // max(rounds, 1))
+    done = 0
+    for r in range(max(rounds, 1)):
+        n_ep = per_round if r < rounds - 1 else epochs - done
+        if r > 0:
+            pred = net.forward(X)
+            for i, d in enumerate(disp):
+                p = pred[i * N:(i + 1) * N]
+                m = d.copy()
+                m[:, 2] = -m[:, 2]
+                Y[i * N:(i + 1) * N] = d if ((p - d) ** 2).sum() <= ((p - m) ** 2).sum() else m
+        net.set_data(X, Y)
+        losses += list(net.train(n_ep, batch=batch, lr=lr, seed=seed + r))
+        done += n_ep
+    return np.array(losses)
+
+
 def predict_positions(net: Mlp, model, f: Field) -> np.ndarray:
     ref = model.dofs(0).reshape(3, -1).T
     d = net.forward(node_features(ref[:, :2], f))
@@ -253,14 +284,13 @@ def main(argv=None):
                 report["train_not_done"] += 1
     report["datagen_s"] = time.time() - t0
     report["train_steps_mean"] = float(np.mean(steps))
-    X, Y = dataset(model, kept, finals)
     net = Mlp(N_FEATURES, width=a.width, hidden_layers=a.hidden, out_dim=3, seed=7)
-    net.set_data(X, Y)
     t0 = time.time()
-    losses = net.train(a.epochs, batch=a.batch, lr=a.lr, seed=1)
+    losses = train_network(net, model, kept, finals, a.epochs, batch=a.batch, lr=a.lr)
     train_s = time.time() - t0
-    flops = 3.0 * network_flops_per_row(N_FEATURES, a.width, a.hidden) * X.shape[0] * a.epochs
-    report.update({"rows": int(X.shape[0]), "train_s": train_s, "train_tflops": flops / train_s / 1e12,
+    rows = len(kept) * model.num_nodes
+    flops = 3.0 * network_flops_per_row(N_FEATURES, a.width, a.hidden) * rows * a.epochs
+    report.update({"rows": int(rows), "train_s": train_s, "train_tflops": flops / train_s / 1e12,
                    "loss_first": float(losses[0]), "loss_last": float(losses[-1])})
     report["eval"] = evaluate(net, model, held_f, prec, a.max_steps)
     with open(a.out, "w") as f:

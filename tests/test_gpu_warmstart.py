@@ -33,10 +33,8 @@ def test_learned_start_beats_plain_start(workdir):
     held = warmstart.fields(8, seed=12)
     finals, steps, status, _ = warmstart.solve(m, train)
     assert (status == 3).all(), status
-    X, Y = warmstart.dataset(m, train, finals)
     net = Mlp(warmstart.N_FEATURES, width=128, hidden_layers=3, out_dim=3, seed=1)
-    net.set_data(X, Y)
-    losses = net.train(epochs=150, batch=4096, lr=2e-3, seed=0)
+    losses = warmstart.train_network(net, m, train, finals, epochs=300, batch=4096, lr=2e-3, rounds=3)
     assert losses[-1] < 0.3 * losses[0], losses[[0, -1]]
     r = warmstart.evaluate(net, m, held)
     assert r["plain_done"] == 8 and r["learned_done"] == 8, r

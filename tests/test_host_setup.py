@@ -176,3 +176,20 @@ def test_model_from_arrays_equals_file(workdir):
         else:
             assert np.array_equal(t1[k], t2[k]), k
     assert abs(m1.scalars.timestep - m2.scalars.timestep) <= 1e-13 * m1.scalars.timestep
+
+
+def test_parallel_setup_matches_serial(tmp_path, monkeypatch):
+    """The per-triangle set-up loops run in threads on larger meshes; the
+    tables are identical to a one-thread run."""
+    from morphoshell_b200 import Model, meshgen
+    mesh, info, bbar = meshgen.workload("disk12")
+    st = str(tmp_path / "s.txt")
+    meshgen.write_settings(st, protocol=3)
+    out = []
+    for threads in ("1", "7"):
+        monkeypatch.setenv("MORPHOSHELL_SETUP_THREADS", threads)
+        m = Model.from_arrays(st, mesh.nodes, mesh.tris, info, bbar)
+        assert m.num_tris > 4096
+        out.append(m.tables())
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k
