@@ -273,8 +273,9 @@ typedef struct ms_batch_inst_status {
     int64_t offending_dof;     /* failed: dof (SoA, within the instance) whose force tripped the guard, else -1 */
 } ms_batch_inst_status;
 
-/* Launch schedule: threads per block of the per-triangle and per-node
- * kernels, steps per captured graph (even). */
+/* Launch schedule: threads per block of the per-triangle kernel (0: the
+ * persistent kernel fed by bulk-copied 128-triangle tiles, the default) and
+ * of the per-node kernel, steps per captured graph (even). */
 typedef struct ms_batch_schedule {
     int32_t tri_block, node_block, chunk_steps;
 } ms_batch_schedule;

@@ -30,6 +30,7 @@
 #include "../../../include/morphoshell_gpu.h"
 #include "internal.cuh"
 #include "step_common.cuh"
+#include "tile_copy.cuh"
 #include "tri_contrib.cuh"
 
 namespace msb {
@@ -106,6 +107,47 @@ __global__ void __launch_bounds__(BLOCK) k_batch_tri(const DevMesh m, const Clus
     if constexpr (MIXED) out = m.contrib_f + (size_t)t0 * 18;
     else out = s.contrib + (size_t)t0 * 18;
     for (int j = lane; j < total; j += 32) out[j] = sw[j];
+}
+
+// The same contributions from bulk-copied tile records (tile_copy.cuh),
+// persistent blocks; tri_inst[t] is the triangle's instance.
+template <bool MIXED>
+__global__ void __launch_bounds__(kTile) k_batch_tri_tiles(const DevMesh m, const ClusterPlan p, const DevState s,
+                                                         const int* __restrict__ tri_inst,
+                                                         const InstParams* __restrict__ ip,
+                                                         const InstState* __restrict__ is, int* err, int parity) {
+    using R = typename Real<MIXED>::T;
+    const double* pos = pos_buf(s, parity);
+    const unsigned char* tl = reinterpret_cast<const unsigned char*>(MIXED ? p.tiles_f : p.tiles);
+    R* out;
+    if constexpr (MIXED) out = m.contrib_f;
+    else out = s.contrib;
+    tiles::tile_loop<MIXED>(
+        m.T, tl, out, err,
+        [&](int t, const int (&ids)[6], const R (&c)[24], double area, double c2, double s2, double cs, R (&f)[18]) {
+            const int inst = __ldg(tri_inst + t);
+            const InstState& st = is[inst];
+            if (is_frozen(st.status)) return;
+            const InstParams& q = ip[inst];
+            TriMat<double> mt;
+            if (q.uniform_hmu) {
+                mt.h = q.h;
+                mt.mu = q.mu;
+            } else {
+                mt.h = __ldg(m.thick + t);
+                mt.mu = __ldg(m.shear + t);
+            }
+            mt.area = area;
+            lce_metric(c2, s2, cs, st.cur_lam * st.cur_lam, st.cur_pw, mt);
+            double P[6][3];
+#pragma unroll
+            for (int sl = 0; sl < 6; ++sl) {
+                P[sl][0] = __ldg(pos + ids[sl]);
+                P[sl][1] = __ldg(pos + m.N + ids[sl]);
+                P[sl][2] = __ldg(pos + 2 * m.N + ids[sl]);
+            }
+            tri_forces<MIXED>(P, c, mt, q.nu, q.gamma, f);
+        });
 }
 
 template <bool MIXED, int BLOCK>
@@ -228,7 +270,9 @@ __global__ void __launch_bounds__(kPostBlock) k_batch_post(const InstParams* __r
 struct Sched {
     int tri_block, node_block;
 };
-constexpr Sched kScheds[] = {{128, 256}, {64, 256}, {256, 256}, {128, 128}, {64, 128}, {256, 128}, {128, 512}};
+// tri_block 0: the persistent bulk-copy tile kernel.
+constexpr Sched kScheds[] = {{0, 256},   {128, 256}, {64, 256}, {256, 256}, {128, 128},
+                             {64, 128},  {256, 128}, {128, 512}, {0, 128}};
 constexpr int kNumScheds = sizeof(kScheds) / sizeof(kScheds[0]);
 
 template <bool MIXED>
@@ -293,6 +337,9 @@ struct ms_batch {
     double* d_fnorm = nullptr;
     double* d_vnorm = nullptr;
     InstState* h_is = nullptr;  // pinned mirror
+    int* d_tri_inst = nullptr;   // [T]
+    int* d_err = nullptr;        // copy-wait timeouts of the tile kernel
+    int tile_grid = 0;           // 0: tile kernel unavailable
     int parity = 0;
     int sched = 0;
     int chunk = 64;
@@ -354,7 +401,23 @@ ms_status launch_step(ms_batch* b, int parity, int sched) {
     const int n = b->n_inst;
     k_batch_pre<<<(n + 127) / 128, 128, 0, st>>>(b->d_ip, b->d_is, n);
     cudaError_t e;
-    if (b->precision == MS_PRECISION_MIXED) {
+    if (sc.tri_block == 0) {
+        const int ntiles = (b->m.T + kTile - 1) / kTile;
+        const int grid = std::min(ntiles, b->tile_grid);
+        if (b->precision == MS_PRECISION_MIXED)
+            k_batch_tri_tiles<true><<<grid, kTile, 2 * tiles::TileLayout<true>::bytes, st>>>(
+                b->m, b->p, b->s, b->d_tri_inst, b->d_ip, b->d_is, b->d_err, parity);
+        else
+            k_batch_tri_tiles<false><<<grid, kTile, 2 * tiles::TileLayout<false>::bytes, st>>>(
+                b->m, b->p, b->s, b->d_tri_inst, b->d_ip, b->d_is, b->d_err, parity);
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = b->precision == MS_PRECISION_MIXED
+                    ? launch_node<true>(sc.node_block, b->m, b->s, b->d_node_inst, b->d_ip, b->d_is, b->d_fnorm,
+                                        b->d_vnorm, parity, st)
+                    : launch_node<false>(sc.node_block, b->m, b->s, b->d_node_inst, b->d_ip, b->d_is, b->d_fnorm,
+                                         b->d_vnorm, parity, st);
+    } else if (b->precision == MS_PRECISION_MIXED) {
         e = launch_tri<true>(sc.tri_block, b->m, b->p, b->s, b->d_ip, b->d_is, parity, st);
         if (e == cudaSuccess)
             e = launch_node<true>(sc.node_block, b->m, b->s, b->d_node_inst, b->d_ip, b->d_is, b->d_fnorm,
@@ -406,7 +469,10 @@ bool all_frozen(const ms_batch* b) {
 
 ms_status fetch_states(ms_batch* b) {
     MB_CUDA(b, cudaMemcpyAsync(b->h_is, b->d_is, sizeof(InstState) * b->n_inst, cudaMemcpyDeviceToHost, b->stream));
+    int e = 0;
+    if (b->d_err) MB_CUDA(b, cudaMemcpyAsync(&e, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
     MB_CUDA(b, cudaStreamSynchronize(b->stream));
+    if (e) return bfail(b, MS_ERR_TIMEOUT, "a tile copy did not land within its bounded wait");
     return MS_OK;
 }
 
@@ -615,6 +681,60 @@ ms_status ms_batch_create(const ms_batch_instance* inst, int32_t n, int32_t devi
     p.tri_idx = d_idx;
     p.tri_aux = d_aux;
     p.lce_uniform = 1;
+    // Tile records for the bulk-copy tile kernel (the default schedule).
+    {
+        const int mixed = precision == MS_PRECISION_MIXED;
+        int blocks = 0;
+        cudaError_t ea = mixed ? cudaFuncSetAttribute(k_batch_tri_tiles<true>,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      2 * tiles::TileLayout<true>::bytes)
+                               : cudaFuncSetAttribute(k_batch_tri_tiles<false>,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      2 * tiles::TileLayout<false>::bytes);
+        if (ea == cudaSuccess)
+            ea = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_batch_tri_tiles<true>, kTile,
+                                                                       2 * tiles::TileLayout<true>::bytes)
+                       : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_batch_tri_tiles<false>, kTile,
+                                                                       2 * tiles::TileLayout<false>::bytes);
+        if (ea == cudaSuccess && blocks > 0) {
+            const size_t rec = mixed ? tiles::TileLayout<true>::bytes : tiles::TileLayout<false>::bytes;
+            const long long ntiles = (T + kTile - 1) / kTile;
+            std::vector<unsigned char> buf(rec * ntiles, 0);
+            const size_t ids_b = 6 * kTile * 4, coef_b = 24 * kTile * (mixed ? 4 : 8);
+            std::vector<int> tri_inst(T);
+            for (long long t = 0; t < T; ++t) {
+                const long long tile = t / kTile, li = t % kTile;
+                unsigned char* r = buf.data() + rec * tile;
+                int32_t* ids = reinterpret_cast<int32_t*>(r);
+                double* ax = reinterpret_cast<double*>(r + ids_b + coef_b);
+                for (int k = 0; k < 6; ++k) ids[k * kTile + li] = idx[8ULL * t + k];
+                if (mixed) {
+                    float* c = reinterpret_cast<float*>(r + ids_b);
+                    for (int k = 0; k < 24; ++k) c[k * kTile + li] = mcoef[24ULL * t + k];
+                } else {
+                    double* c = reinterpret_cast<double*>(r + ids_b);
+                    for (int k = 0; k < 24; ++k) c[k * kTile + li] = coef[24ULL * t + k];
+                }
+                for (int k = 0; k < 4; ++k) ax[k * kTile + li] = aux[4ULL * t + k];
+                tri_inst[t] = idx[8ULL * t + 7];
+            }
+            unsigned char* d_tiles;
+            if ((st = bupload(b, &d_tiles, buf)) || (st = bupload(b, &b->d_tri_inst, tri_inst)) ||
+                (st = balloc(b, &b->d_err, 1)))
+                return bail(st);
+            if (cudaMemset(b->d_err, 0, sizeof(int)) != cudaSuccess) return bail(MS_ERR_CUDA);
+            if (mixed) p.tiles_f = d_tiles;
+            else p.tiles = d_tiles;
+            int dev = 0, sms = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            b->tile_grid = sms * blocks;
+        } else {
+            cudaGetLastError();
+            b->tile_grid = 0;
+        }
+        b->sched = b->tile_grid > 0 ? 0 : 1;
+    }
     m.mass = d_mass;
     m.fixed = d_fixed;
     m.inc_off = d_off;
@@ -755,7 +875,8 @@ ms_status ms_batch_set_schedule(ms_batch* b, const ms_batch_schedule* s) {
     if (s->chunk_steps <= 0 || s->chunk_steps % 2 || s->chunk_steps > 1024)
         return bfail(b, MS_ERR_INVALID_ARGUMENT, "chunk_steps must be even, 2..1024");
     for (int k = 0; k < kNumScheds; ++k)
-        if (kScheds[k].tri_block == s->tri_block && kScheds[k].node_block == s->node_block) {
+        if (kScheds[k].tri_block == s->tri_block && kScheds[k].node_block == s->node_block &&
+            (s->tri_block != 0 || b->tile_grid > 0)) {
             b->sched = k;
             b->chunk = s->chunk_steps;
             return MS_OK;
@@ -816,6 +937,7 @@ ms_status ms_batch_autotune(ms_batch* b, int32_t steps, ms_batch_schedule* chose
     };
     if (copy_state(true) != cudaSuccess) rc = bcuda(b, cudaGetLastError(), "autotune save");
     for (int k = 0; k < kNumScheds && rc == MS_OK; ++k) {
+        if (kScheds[k].tri_block == 0 && b->tile_grid == 0) continue;
         // one untimed pass (graph instantiation, caches), then the timed one
         for (int rep = 0; rep < 2 && rc == MS_OK; ++rep) {
             if (copy_state(false) != cudaSuccess) {

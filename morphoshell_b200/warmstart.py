@@ -15,9 +15,12 @@ damped dynamics begin from.
 * Network: ms_mlp_* (tensor-core BF16 SiLU MLP, FP32 accumulation, Adam).
 * Warm start: predicted positions uploaded into a batch instance that waits
   for equilibrium at dial factor 1 (ms_batch_set_start).  The plain damped
-  dynamics always run from there to full equilibrium and judge the start;
-  a prediction that is not finite or whose elastic energy at dial factor 1
-  exceeds the flat start's falls back to the plain start.
+  dynamics always run from there to full equilibrium and judge the start:
+  a prediction that is not finite, or whose run trips the force guard or
+  does not reach equilibrium, falls back to the plain start (optionally
+  also one with more elastic energy at dial factor 1 than the flat start;
+  a flat start is a stressed saddle whose energy is low next to a
+  prediction with small-scale errors, so that test rejects useful starts).
 """
 from __future__ import annotations
 
@@ -29,7 +32,7 @@ import numpy as np
 
 from . import MS_INST_DONE, MS_INST_FAILED, MS_PRECISION_FP64, Batch, GpuLoop, Mlp
 
-N_FEATURES = 23
+N_FEATURES = 22
 
 
 @dataclass
@@ -61,20 +64,21 @@ def abar_info(model_tris_centroids: np.ndarray, f: Field) -> np.ndarray:
 
 
 def node_features(xy: np.ndarray, f: Field) -> np.ndarray:
-    """Per-node inputs: x, y, r, the programmed metric at dial factor 1 at the
-    node (3 components), lambda_final, sin/cos k theta (k = 1..4), and the
-    field's coefficients a_k cos phi_k, a_k sin phi_k (k = 1..4)."""
+    """Per-node inputs, all continuous at the disk's centre (where theta is
+    undefined and the director has its defect): x, y, r, the harmonic
+    polynomials r^k cos k theta, r^k sin k theta (k = 1..4), the director
+    angle alpha as r cos 2 alpha, r sin 2 alpha (the programmed metric
+    depends on 2 alpha), lambda_final, and the field's coefficients
+    a_k cos phi_k, a_k sin phi_k (k = 1..4)."""
     x, y = xy[:, 0], xy[:, 1]
+    r = np.hypot(x, y)
     theta = np.arctan2(y, x)
-    ang = f.angle(theta)
-    c, s = np.cos(ang), np.sin(ang)
-    lam2, p = f.lam ** 2, f.lam ** (-1.0)
-    a0 = lam2 * c * c + p * s * s
-    a1 = (lam2 - p) * c * s
-    a2 = p * c * c + lam2 * s * s
-    cols = [x, y, np.hypot(x, y), a0, a1, a2, np.full_like(x, f.lam)]
+    alpha = f.angle(theta)
+    cols = [x, y, r]
     for k in range(1, 5):
-        cols += [np.sin(k * theta), np.cos(k * theta)]
+        rk = r ** k
+        cols += [rk * np.cos(k * theta), rk * np.sin(k * theta)]
+    cols += [r * np.cos(2 * alpha), r * np.sin(2 * alpha), np.full_like(x, f.lam)]
     for k in range(4):
         cols += [np.full_like(x, f.a[k] * math.cos(f.phi[k])), np.full_like(x, f.a[k] * math.sin(f.phi[k]))]
     return np.column_stack(cols).astype(np.float32)
@@ -186,25 +190,41 @@ def elastic_energy(model, f: Field, x: np.ndarray) -> float:
     return float(e[0] + e[1])
 
 
-def warm_starts(net: Mlp, model, flds):
+def warm_starts(net: Mlp, model, flds, energy_check: bool = False):
     """Predicted start per field, or None (plain start) when the prediction
-    is not finite or has more elastic energy than the flat start."""
+    is not finite (or, with energy_check, has more elastic energy at dial
+    factor 1 than the flat start)."""
     flat = model.dofs(1)
     out, fell_back = [], 0
     for f in flds:
         x = predict_positions(net, model, f)
-        ok = np.all(np.isfinite(x)) and elastic_energy(model, f, x) <= elastic_energy(model, f, flat)
+        ok = bool(np.all(np.isfinite(x)))
+        if ok and energy_check:
+            ok = elastic_energy(model, f, x) <= elastic_energy(model, f, flat)
         out.append(x if ok else None)
         fell_back += 0 if ok else 1
     return out, fell_back
 
 
-def evaluate(net: Mlp, model, flds, precision=MS_PRECISION_FP64, max_steps=2_000_000):
+def evaluate(net: Mlp, model, flds, precision=MS_PRECISION_FP64, max_steps=2_000_000, energy_check: bool = False):
     """Time to the first equilibrium at dial factor 1 from the plain start
-    and from the learned start, and the distance between the two shapes."""
+    and from the learned start, and the distance between the two shapes.
+    The plain dynamics run from every learned start; a start whose run
+    trips the force guard or does not reach equilibrium within max_steps
+    falls back to the plain start, and its time is the learned attempt plus
+    the plain run."""
     plain, s_plain, st_plain, w_plain = solve(model, flds, precision, None, max_steps)
-    starts, fell_back = warm_starts(net, model, flds)
-    learned, s_learn, st_learn, w_learn = solve(model, flds, precision, starts, max_steps)
+    starts, fell_back = warm_starts(net, model, flds, energy_check)
+    budget = min(max_steps, int(2 * s_plain.max()) + 1000)
+    learned, s_learn, st_learn, w_learn = solve(model, flds, precision, starts, budget)
+    s_total = s_learn.astype(np.float64).copy()
+    for i, st in enumerate(st_learn):
+        if st != MS_INST_DONE:
+            fell_back += 1
+            learned[i] = plain[i]
+            s_total[i] = s_learn[i] + s_plain[i]
+        elif starts[i] is None:
+            s_total[i] = s_plain[i]
     dist = []
     for a, b in zip(plain, learned):
         da, db = a.reshape(3, -1), b.reshape(3, -1)
@@ -213,8 +233,9 @@ def evaluate(net: Mlp, model, flds, precision=MS_PRECISION_FP64, max_steps=2_000
         dist.append(min(np.abs(da - db).max(), np.abs(da - mirrored).max()))
     return {
         "fields": len(flds), "fell_back": fell_back,
-        "plain_steps_mean": float(s_plain.mean()), "learned_steps_mean": float(s_learn.mean()),
-        "step_speedup": float(s_plain.mean() / max(s_learn.mean(), 1.0)),
+        "plain_steps_mean": float(s_plain.mean()), "learned_steps_mean": float(s_total.mean()),
+        "step_speedup": float(s_plain.mean() / max(s_total.mean(), 1.0)),
+        "step_speedup_median": float(np.median(s_plain / np.maximum(s_total, 1.0))),
         "plain_wall_s": w_plain, "learned_wall_s": w_learn, "wall_speedup": w_plain / max(w_learn, 1e-9),
         "plain_done": int((st_plain == MS_INST_DONE).sum()), "learned_done": int((st_learn == MS_INST_DONE).sum()),
         "failed": int((st_plain == MS_INST_FAILED).sum() + (st_learn == MS_INST_FAILED).sum()),
