@@ -110,15 +110,21 @@ __device__ __forceinline__ void eq_block_reduce_and_finish(const DevState& s, do
     eq_store_and_fold(s, r, blockIdx.x, gridDim.x, gridDim.x);
 }
 
+// Resident blocks the node kernel asks the compiler for: the FP64 gather
+// holds more in flight per thread and is best unconstrained (64 registers);
+// the mixed one is best at 48 registers, five blocks per SM (measured).
 #ifndef MSB_NODE_MINB
 #define MSB_NODE_MINB 1
+#endif
+#ifndef MSB_NODE_MINB_MIXED
+#define MSB_NODE_MINB_MIXED 5
 #endif
 #ifndef MSB_NODE_REVERSE
 #define MSB_NODE_REVERSE 1
 #endif
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kNodeBlock, MSB_NODE_MINB)
+__global__ void __launch_bounds__(kNodeBlock, MIXED ? MSB_NODE_MINB_MIXED : MSB_NODE_MINB)
     k_node_update(const DevMesh m, const DevState s, const StepScalars sc) {
     const int gstep = global_step(s.err, sc.step);
     if (stale(s.err, gstep)) return;  // uniform: only earlier kernels can make it true

@@ -122,6 +122,28 @@ def solve(model, flds, precision=MS_PRECISION_FP64, starts=None, max_steps=2_000
     return out, np.array(steps), np.array(stat), wall
 
 
+def align(P: np.ndarray, Q: np.ndarray) -> np.ndarray:
+    """P (N, 3) moved by the proper rigid motion that best matches it to Q
+    in the least-squares sense (Kabsch).  Equilibria are defined up to
+    rigid motions, and the damped dynamics of an unconstrained sheet drift
+    and turn it."""
+    pc, qc = P.mean(0), Q.mean(0)
+    H = (P - pc).T @ (Q - qc)
+    U, _, Vt = np.linalg.svd(H)
+    d = np.sign(np.linalg.det(Vt.T @ U.T))
+    D = np.diag([1.0, 1.0, d])
+    R = Vt.T @ D @ U.T
+    return (P - pc) @ R.T + qc
+
+
+def shape_distance(a: np.ndarray, b: np.ndarray) -> float:
+    """Largest node distance between two shapes (3N SoA) after the best
+    rigid motion, allowing b's mirror image z -> -z."""
+    A, B = a.reshape(3, -1).T, b.reshape(3, -1).T
+    Bm = B * np.array([1.0, 1.0, -1.0])
+    return float(min(np.abs(align(B, A) - A).max(), np.abs(align(Bm, A) - A).max()))
+
+
 def canonical(disp: np.ndarray) -> np.ndarray:
     """(N, 3) displacement mirrored so that its mean z is >= 0."""
     d = disp.copy()
@@ -136,7 +158,7 @@ def dataset(model, flds, finals):
     X, Y = [], []
     for f, x in zip(flds, finals):
         X.append(node_features(xy, f))
-        Y.append(canonical(x.reshape(3, -1).T - ref).astype(np.float32))
+        Y.append(canonical(align(x.reshape(3, -1).T, ref) - ref).astype(np.float32))
     return np.concatenate(X), np.concatenate(Y)
 
 
@@ -151,7 +173,7 @@ def train_network(net: Mlp, model, flds, finals, epochs: int, batch: int = 8192,
     xy = ref[:, :2]
     N = ref.shape[0]
     X = np.concatenate([node_features(xy, f) for f in flds])
-    disp = [x.reshape(3, -1).T - ref for x in finals]
+    disp = [align(x.reshape(3, -1).T, ref) - ref for x in finals]
     Y = np.concatenate([canonical(d) for d in disp]).astype(np.float32)
     losses = []
     per_round = max(1, epochs // max(rounds, 1))
@@ -225,12 +247,7 @@ def evaluate(net: Mlp, model, flds, precision=MS_PRECISION_FP64, max_steps=2_000
             s_total[i] = s_learn[i] + s_plain[i]
         elif starts[i] is None:
             s_total[i] = s_plain[i]
-    dist = []
-    for a, b in zip(plain, learned):
-        da, db = a.reshape(3, -1), b.reshape(3, -1)
-        mirrored = db.copy()
-        mirrored[2] = -mirrored[2]
-        dist.append(min(np.abs(da - db).max(), np.abs(da - mirrored).max()))
+    dist = [shape_distance(a, b) for a, b in zip(plain, learned)]
     return {
         "fields": len(flds), "fell_back": fell_back,
         "plain_steps_mean": float(s_plain.mean()), "learned_steps_mean": float(s_total.mean()),
