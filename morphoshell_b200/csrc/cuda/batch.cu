@@ -69,7 +69,8 @@ __global__ void __launch_bounds__(BLOCK) k_batch_tri(const DevMesh m, const Clus
                                                      const InstParams* __restrict__ ip,
                                                      const InstState* __restrict__ is, int parity) {
     using R = typename Real<MIXED>::T;
-    __shared__ R stage[BLOCK * 18];
+    constexpr int CS = contrib_stride<MIXED>();
+    __shared__ R stage[BLOCK * CS];
     const int t = blockIdx.x * BLOCK + threadIdx.x;
     const bool live = t < m.T;
     R f[18];
@@ -97,15 +98,14 @@ __global__ void __launch_bounds__(BLOCK) k_batch_tri(const DevMesh m, const Clus
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (!__any_sync(0xffffffffu, live)) return;
-    R* sw = stage + warp * 32 * 18;
-#pragma unroll
-    for (int j = 0; j < 18; ++j) sw[lane * 18 + j] = f[j];
+    R* sw = stage + warp * 32 * CS;
+    stage_contrib<MIXED>(sw + lane * CS, f);
     __syncwarp();
     const int t0 = t - lane;
-    const int total = min(32, m.T - t0) * 18;
+    const int total = min(32, m.T - t0) * CS;
     R* out;
-    if constexpr (MIXED) out = m.contrib_f + (size_t)t0 * 18;
-    else out = s.contrib + (size_t)t0 * 18;
+    if constexpr (MIXED) out = m.contrib_f + (size_t)t0 * CS;
+    else out = s.contrib + (size_t)t0 * CS;
     for (int j = lane; j < total; j += 32) out[j] = sw[j];
 }
 
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(kTile) k_batch_tri_tiles(const DevMesh m, cons
                 mt.mu = __ldg(m.shear + t);
             }
             mt.area = area;
-            lce_metric(c2, s2, cs, st.cur_lam * st.cur_lam, st.cur_pw, mt);
+            lce_metric(c2, s2, cs, __dmul_rn(st.cur_lam, st.cur_lam), st.cur_pw, mt);
             double P[6][3];
 #pragma unroll
             for (int sl = 0; sl < 6; ++sl) {
@@ -669,7 +669,7 @@ ms_status ms_batch_create(const ms_batch_instance* inst, int32_t n, int32_t devi
         return bail(st);
     if (precision == MS_PRECISION_MIXED) {
         float *d_mc, *d_cf;
-        if ((st = bupload(b, &d_mc, mcoef)) || (st = balloc(b, &d_cf, 18ULL * T))) return bail(st);
+        if ((st = bupload(b, &d_mc, mcoef)) || (st = balloc(b, &d_cf, 6ULL * kMixedSlot * T))) return bail(st);
         p.coef_aos_f = d_mc;
         m.contrib_f = d_cf;
     } else {

@@ -544,7 +544,7 @@ ms_status ms_create(const ms_mesh_desc* d, const ms_params* prm, int device, int
         return bail(st);
     if (precision == MS_PRECISION_MIXED) {
         float* contrib_f;
-        if ((st = dalloc(h, &contrib_f, 18ULL * T))) return bail(st);
+        if ((st = dalloc(h, &contrib_f, 6ULL * kMixedSlot * T))) return bail(st);
         m.contrib_f = contrib_f;
     }
     h->area_host.assign(d->ref_area, d->ref_area + T);

@@ -84,10 +84,11 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int slot = 0; slot < 6; ++slot)
                 if (halo_mask & (1 << slot)) {
                     if constexpr (MIXED) {
-                        float* o = m.contrib_f + 3 * (6 * (size_t)t + slot);
+                        float* o = m.contrib_f + kMixedSlot * (6 * (size_t)t + slot);
                         o[0] = (float)f[3 * slot];
                         o[1] = (float)f[3 * slot + 1];
                         o[2] = (float)f[3 * slot + 2];
+                        if (kMixedSlot == 4) o[3] = 0.0f;
                     } else {
                         double* o = s.contrib + 3 * (6 * (size_t)t + slot);
                         o[0] = (double)f[3 * slot];
@@ -141,7 +142,8 @@ template <int DIAL, bool MIXED>
 __global__ void __launch_bounds__(kAosBlock, MSB_TRI_MINB)
     k_tri_aos(const DevMesh m, const ClusterPlan p, const DevState s, const StepScalars sc) {
     using R = typename Real<MIXED>::T;
-    __shared__ R stage[kAosBlock * 18];
+    constexpr int CS = contrib_stride<MIXED>();
+    __shared__ R stage[kAosBlock * CS];
     const int gstep = global_step(s.err, sc.step);
     if (stale(s.err, gstep)) return;  // uniform over the grid
     const int t = blockIdx.x * kAosBlock + threadIdx.x;
@@ -166,15 +168,14 @@ __global__ void __launch_bounds__(kAosBlock, MSB_TRI_MINB)
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (!__any_sync(0xffffffffu, live)) return;
-    R* sw = stage + warp * 32 * 18;
-#pragma unroll
-    for (int j = 0; j < 18; ++j) sw[lane * 18 + j] = f[j];
+    R* sw = stage + warp * 32 * CS;
+    stage_contrib<MIXED>(sw + lane * CS, f);
     __syncwarp();
     const int t0 = t - lane;
-    const int total = min(32, m.T - t0) * 18;
+    const int total = min(32, m.T - t0) * CS;
     R* out;
-    if constexpr (MIXED) out = m.contrib_f + (size_t)t0 * 18;
-    else out = s.contrib + (size_t)t0 * 18;
+    if constexpr (MIXED) out = m.contrib_f + (size_t)t0 * CS;
+    else out = s.contrib + (size_t)t0 * CS;
     for (int j = lane; j < total; j += 32) out[j] = sw[j];
 }
 
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(kHaloBlock)
         for (int k = b; k < e; ++k) {
             const size_t en = (size_t)__ldg(m.inc_ent + k);
             if constexpr (MIXED) {
-                const float* c = m.contrib_f + 3 * en;
+                const float* c = m.contrib_f + kMixedSlot * en;
                 Fx += (double)c[0];
                 Fy += (double)c[1];
                 Fz += (double)c[2];

@@ -126,6 +126,22 @@ struct ClusterPlan {
 // Triangles per tile of the bulk-copy-fed per-triangle kernel.
 constexpr int kTile = 128;
 
+// Layout of the per-(triangle, slot) force contributions: x, y, z doubles;
+// for the mixed path x, y, z floats, optionally padded with a zero to 16
+// bytes so that the node kernel loads each with one vector load.
+#ifndef MSB_MIXED_PAD4
+#define MSB_MIXED_PAD4 0
+#endif
+constexpr int kMixedSlot = MSB_MIXED_PAD4 ? 4 : 3;
+template <bool MIXED>
+__host__ __device__ constexpr int contrib_slot() {
+    return MIXED ? kMixedSlot : 3;
+}
+template <bool MIXED>
+__host__ __device__ constexpr int contrib_stride() {
+    return 6 * contrib_slot<MIXED>();
+}
+
 // ---- batched ensembles (batch.cu) ----------------------------------------------
 // Many meshes stepped together: their tables are concatenated into one union
 // mesh (nodes and triangles of instance i contiguous), every triangle and

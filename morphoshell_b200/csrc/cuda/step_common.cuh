@@ -4,6 +4,7 @@
 #pragma once
 
 #include <climits>
+#include <type_traits>
 
 #include "internal.cuh"
 
@@ -177,13 +178,21 @@ __device__ __forceinline__ void gather_sell(const DevMesh& m, const Cf* __restri
 #pragma unroll
         for (int j = 0; j < kNodeBatch; ++j) ei[j] = (k + j < width) ? __ldg(ep + 32 * (k + j)) : -1;
         Cf v[kNodeBatch][3];
+        constexpr int S = std::is_same<Cf, float>::value ? kMixedSlot : 3;
 #pragma unroll
         for (int j = 0; j < kNodeBatch; ++j) {
             if (ei[j] >= 0) {
-                const Cf* q = c + 3 * (size_t)ei[j];
-                v[j][0] = q[0];
-                v[j][1] = q[1];
-                v[j][2] = q[2];
+                const Cf* q = c + S * (size_t)ei[j];
+                if constexpr (S == 4) {
+                    const float4 w = __ldg(reinterpret_cast<const float4*>(q));
+                    v[j][0] = w.x;
+                    v[j][1] = w.y;
+                    v[j][2] = w.z;
+                } else {
+                    v[j][0] = q[0];
+                    v[j][1] = q[1];
+                    v[j][2] = q[2];
+                }
             }
         }
 #pragma unroll

@@ -18,7 +18,8 @@ struct TileLayout {
     static constexpr int aux = 4 * kTile * 8;
     static constexpr int bytes = ids + coef + aux;
     static_assert(bytes % 16 == 0, "bulk copies move multiples of 16 bytes");
-    static_assert(coef >= kTile * 18 * (MIXED ? 4 : 8), "the weight area holds a tile's contributions");
+    static_assert(coef >= kTile * contrib_stride<MIXED>() * (MIXED ? 4 : 8),
+                  "the weight area holds a tile's contributions");
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
@@ -62,7 +63,7 @@ __device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity) {
 // a double buffer with one bulk copy while the block works on the current
 // one.  For each triangle t < T, body(t, ids, c, area, c2, s2, cs, f) fills
 // its 18 contributions f; they leave through the consumed weight area as
-// contiguous runs to out[18 t ...].  Returns false, with *err_flag set to
+// contiguous runs to out[contrib_stride t ...].  Returns false, with *err_flag set to
 // 5 (MS_ERR_TIMEOUT) when it was 0, if a copy did not land within the
 // bounded wait.
 template <bool MIXED, typename Body>
@@ -119,13 +120,13 @@ __device__ __forceinline__ bool tile_loop(int T, const unsigned char* __restrict
 #pragma unroll
         for (int j = 0; j < 18; ++j) f[j] = R(0);
         if (t < T) body(t, ids, c, area, c2, s2, cs, f);
-        R* sw = scoef + warp * 32 * 18;
-#pragma unroll
-        for (int j = 0; j < 18; ++j) sw[lane * 18 + j] = f[j];
+        constexpr int CS = contrib_stride<MIXED>();
+        R* sw = scoef + warp * 32 * CS;
+        tridev::stage_contrib<MIXED>(sw + lane * CS, f);
         __syncwarp();
         const int t0 = tile * kTile + warp * 32;
-        const int total = max(0, min(32, T - t0)) * 18;
-        R* o = out + (size_t)t0 * 18;
+        const int total = max(0, min(32, T - t0)) * CS;
+        R* o = out + (size_t)t0 * CS;
         for (int j = lane; j < total; j += 32) o[j] = sw[j];
         // Order these generic-proxy writes before the bulk copy that will
         // refill this half.

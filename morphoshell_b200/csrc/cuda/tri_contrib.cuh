@@ -21,6 +21,21 @@ struct Real<true> {
     using T = float;
 };
 
+// One triangle's 18 contributions into its contrib_stride<MIXED>() staging
+// slots (zero padding where the layout has it).
+template <bool MIXED>
+__device__ __forceinline__ void stage_contrib(typename Real<MIXED>::T* __restrict__ dst,
+                                              const typename Real<MIXED>::T (&f)[18]) {
+    using R = typename Real<MIXED>::T;
+    constexpr int S = contrib_slot<MIXED>();
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) dst[S * s + c] = f[3 * s + c];
+        if constexpr (S == 4) dst[S * s + 3] = R(0);
+    }
+}
+
 // Thickness and shear modulus of triangle t.
 __device__ __forceinline__ void tri_hmu(const DevMesh& m, int t, double& h, double& mu) {
     if (m.uniform_hmu) {
@@ -35,11 +50,13 @@ __device__ __forceinline__ void tri_hmu(const DevMesh& m, int t, double& h, doub
 // Protocol-3 programmed metric (do_dialling.cpp:112-123) from the director
 // trigonometry cos^2, sin^2, cos sin and l2 = lambda^2, pp = lambda^(-2 nu_ot);
 // bbar = 0.
+// The roundings are spelled out (fma, then products) so that every kernel
+// that inlines this gets the same bits whatever the compiler would contract.
 __device__ __forceinline__ void lce_metric(double c2, double s2, double cs, double l2, double pp,
                                            TriMat<double>& mt) {
-    mt.abar0 = l2 * c2 + pp * s2;
-    mt.abar1 = (l2 - pp) * cs;
-    mt.abar2 = pp * c2 + l2 * s2;
+    mt.abar0 = __fma_rn(l2, c2, __dmul_rn(pp, s2));
+    mt.abar1 = __dmul_rn(__dsub_rn(l2, pp), cs);
+    mt.abar2 = __fma_rn(pp, c2, __dmul_rn(l2, s2));
     mt.bbar0 = mt.bbar1 = mt.bbar2 = 0.0;
 }
 
@@ -128,10 +145,11 @@ __device__ __forceinline__ void tri_forces(const double (&P)[6][3], const typena
     }
 #pragma unroll
     for (int s = 0; s < 6; ++s) {
-        const R mxx = c[6 + 3 * s + 0], mxy = c[6 + 3 * s + 1], myy = c[6 + 3 * s + 2];
-        R fx = mxx * g.rxx.x + mxy * g.rxy.x + myy * g.ryy.x;
-        R fy = mxx * g.rxx.y + mxy * g.rxy.y + myy * g.ryy.y;
-        R fz = mxx * g.rxx.z + mxy * g.rxy.z + myy * g.ryy.z;
+        // Second-derivative part: sum_k m_k (ab_k n) = (sum_k m_k ab_k) n.
+        const R beta = c[6 + 3 * s + 0] * g.ab[0] + c[6 + 3 * s + 1] * g.ab[1] + c[6 + 3 * s + 2] * g.ab[2];
+        R fx = beta * g.n.x;
+        R fy = beta * g.n.y;
+        R fz = beta * g.n.z;
         if (s < 3) {
             const R dx = c[s], dy = c[3 + s];
             fx += dx * g.rx.x + dy * g.ry.x;
@@ -163,11 +181,11 @@ __device__ __forceinline__ void tri_contrib(const DevMesh& m, const ClusterPlan&
         const double2* ap = reinterpret_cast<const double2*>(p.tri_aux + t);
         const double2 a01 = __ldg(ap), a23 = __ldg(ap + 1);
         mt.area = a01.x;
-        double l2 = lam * lam, pp = pw;
+        double l2 = __dmul_rn(lam, lam), pp = pw;
         if (!p.lce_uniform) {
             const double2 ln = __ldg(p.lce_ln + t);
             const double lt = (1.0 - dial) * 1.0 + dial * ln.x;
-            l2 = lt * lt;
+            l2 = __dmul_rn(lt, lt);
             pp = pow(lt, -2.0 * ln.y);
         }
         lce_metric(a01.y, a23.x, a23.y, l2, pp, mt);

@@ -64,6 +64,10 @@ struct TriMat {
 template <typename R>
 struct CqGrad {
     V3<R> rx, ry, rxx, rxy, ryy;
+    // The three second-derivative gradients are multiples of the unit
+    // normal: dE/dR_ab = ab[k] n (k = xx, xy, yy).
+    R ab[3];
+    V3<R> n;
 };
 
 // Quadratic-form helper: for symmetric D = [[d0, d1], [d1, d2]] and
@@ -170,6 +174,10 @@ __device__ __forceinline__ void energy_gradient_strain(const Cq<R>& c, const Tri
     g.ry = {A * (s1 * c.rx.x + two * s2 * c.ry.x + gxrx.x), A * (s1 * c.rx.y + two * s2 * c.ry.y + gxrx.y),
             A * (s1 * c.rx.z + two * s2 * c.ry.z + gxrx.z)};
     const R Ab0 = -A * be0, Ab1 = -A * be1, Ab2 = -A * be2;
+    g.ab[0] = Ab0;
+    g.ab[1] = Ab1;
+    g.ab[2] = Ab2;
+    g.n = n;
     g.rxx = {Ab0 * n.x, Ab0 * n.y, Ab0 * n.z};
     g.rxy = {Ab1 * n.x, Ab1 * n.y, Ab1 * n.z};
     g.ryy = {Ab2 * n.x, Ab2 * n.y, Ab2 * n.z};

@@ -50,11 +50,11 @@ __global__ void __launch_bounds__(kTile) k_tri_tiles(const DevMesh m, const Clus
                          tri_hmu(m, t, mt.h, mt.mu);
                          mt.area = area;
                          if (DIAL == DIAL_LCE) {
-                             double l2 = lam * lam, pp = pw;
+                             double l2 = __dmul_rn(lam, lam), pp = pw;
                              if (!p.lce_uniform) {
                                  const double2 ln = __ldg(p.lce_ln + t);
                                  const double lt = (1.0 - dial) * 1.0 + dial * ln.x;
-                                 l2 = lt * lt;
+                                 l2 = __dmul_rn(lt, lt);
                                  pp = pow(lt, -2.0 * ln.y);
                              }
                              lce_metric(c2, s2, cs, l2, pp, mt);

@@ -248,6 +248,8 @@ def evaluate(net: Mlp, model, flds, precision=MS_PRECISION_FP64, max_steps=2_000
         elif starts[i] is None:
             s_total[i] = s_plain[i]
     dist = [shape_distance(a, b) for a, b in zip(plain, learned)]
+    e_plain = [elastic_energy(model, f, x) for f, x in zip(flds, plain)]
+    e_learn = [elastic_energy(model, f, x) for f, x in zip(flds, learned)]
     return {
         "fields": len(flds), "fell_back": fell_back,
         "plain_steps_mean": float(s_plain.mean()), "learned_steps_mean": float(s_total.mean()),
@@ -257,6 +259,9 @@ def evaluate(net: Mlp, model, flds, precision=MS_PRECISION_FP64, max_steps=2_000
         "plain_done": int((st_plain == MS_INST_DONE).sum()), "learned_done": int((st_learn == MS_INST_DONE).sum()),
         "failed": int((st_plain == MS_INST_FAILED).sum() + (st_learn == MS_INST_FAILED).sum()),
         "shape_distance_max": float(np.max(dist)), "shape_distance_median": float(np.median(dist)),
+        "same_shape_fraction": float(np.mean(np.array(dist) < 0.05)),
+        "plain_energy_median": float(np.median(e_plain)), "learned_energy_median": float(np.median(e_learn)),
+        "learned_lower_energy_fraction": float(np.mean(np.array(e_learn) <= np.array(e_plain))),
     }
 
 
@@ -307,6 +312,13 @@ def main(argv=None):
     train_f = fields(a.train, seed=100)
     held_f = fields(a.held_out, seed=200)
 
+    import sys as _sys
+
+    def note(msg):
+        print("[warmstart %.0fs] %s" % (time.time() - t_start, msg), file=_sys.stderr, flush=True)
+
+    t_start = time.time()
+    note("model %s: %d nodes, %d triangles" % (a.mesh, model.num_nodes, model.num_tris))
     t0 = time.time()
     finals, steps, kept = [], [], []
     report["train_not_done"] = 0
@@ -320,6 +332,7 @@ def main(argv=None):
                 steps.append(n_steps)
             else:
                 report["train_not_done"] += 1
+        note("solved %d training fields (steps mean %.0f)" % (min(len(train_f), c0 + a.chunk), np.mean(sx)))
     report["datagen_s"] = time.time() - t0
     report["train_steps_mean"] = float(np.mean(steps))
     net = Mlp(N_FEATURES, width=a.width, hidden_layers=a.hidden, out_dim=3, seed=7)
@@ -330,7 +343,9 @@ def main(argv=None):
     flops = 3.0 * network_flops_per_row(N_FEATURES, a.width, a.hidden) * rows * a.epochs
     report.update({"rows": int(rows), "train_s": train_s, "train_tflops": flops / train_s / 1e12,
                    "loss_first": float(losses[0]), "loss_last": float(losses[-1])})
+    note("trained: loss %.3e -> %.3e in %.1fs" % (losses[0], losses[-1], train_s))
     report["eval"] = evaluate(net, model, held_f, prec, a.max_steps)
+    note("evaluated")
     with open(a.out, "w") as f:
         json.dump(report, f, indent=1)
     print(json.dumps(report))
