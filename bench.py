@@ -450,6 +450,52 @@ def run_ensemble(args):
     return 0
 
 
+def run_mlp(args):
+    """``--workload mlp``: training throughput of the warm-start network on
+    the tensor cores (ms_mlp_train: tcgen05 BF16 GEMMs, FP32 accumulation,
+    Adam), 22 -> 256 x 4 (SiLU) -> 3, batches of 32768 rows of 2^20 seeded
+    synthetic rows (the node features' shape; no dataset exists).  A step is
+    one epoch; value = FLOP/s of the forward and backward GEMMs."""
+    import torch
+    from morphoshell_b200 import Mlp, warmstart
+
+    rows = 1 << 20
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal((rows, warmstart.N_FEATURES)).astype(np.float32)
+    t = np.stack([np.sin(x[:, 0]) * np.cos(x[:, 1]), 0.5 * x[:, 2] * x[:, 3], np.tanh(x[:, 4])], 1)
+    net = Mlp(warmstart.N_FEATURES, width=256, hidden_layers=4, out_dim=3, seed=1)
+    net.set_data(x, t.astype(np.float32))
+    net.train(args.warmup, batch=32768, lr=1e-3, seed=0)
+    stream = torch.cuda.ExternalStream(net.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        losses = net.train(args.steps, batch=32768, lr=1e-3, seed=1)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    flops = 3.0 * warmstart.network_flops_per_row(warmstart.N_FEATURES, 256, 4) * rows * args.steps
+    tflops = flops / (ms / 1e3) / 1e12
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak, peak_kind = float(json.load(f)["bf16_tflops_sustained"]), "measured (sustained)"
+    except (OSError, KeyError, ValueError):
+        peak, peak_kind = 1400.0, "fallback"
+    line = {"metric": "TFLOP/s (network training)", "value": tflops, "unit": "TFLOP/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (fp32 accumulate)", "data": "synthetic",
+            "config": {"workload": "mlp: warm-start network 22 -> 256 x 4 -> 3, %d rows per epoch, batch 32768" % rows,
+                       "rows_per_s": rows * args.steps / (ms / 1e3), "loss_last": float(losses[-1])},
+            "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
+                         "frac": tflops / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "k_gemm (tcgen05, the whole training step incl. transposes, Adam, host loss reads)"},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -467,6 +513,8 @@ def main():
         return run_reference(args)
     if args.workload.startswith("ensemble"):
         return run_ensemble(args)
+    if args.workload == "mlp":
+        return run_mlp(args)
     return run_ours(args)
 
 

@@ -95,13 +95,42 @@ __global__ void k_splitk_sum(const float* __restrict__ part, int S, int Mp, int 
     out[i] = s;
 }
 
-// Column sums of a bf16 [B][N] matrix (bias gradients), one thread per column.
-__global__ void k_colsum(const __nv_bfloat16* __restrict__ D, int B, int N, int n_valid, float* __restrict__ out) {
+// Column sums of a bf16 [B][N] matrix (bias gradients) in two fixed-order
+// passes: block (x, y) sums columns 32x .. 32x+31 over rows
+// [y R, (y+1) R) into part[y][c] (8 row lanes, then the lanes in order),
+// then one thread per column adds the partials in order.
+constexpr int kColChunks = 64;
+
+__global__ void k_colsum_part(const __nv_bfloat16* __restrict__ D, int B, int N, float* __restrict__ part) {
+    __shared__ float acc[8][33];
+    const int c = blockIdx.x * 32 + threadIdx.x;
+    const int R = (B + kColChunks - 1) / kColChunks;
+    const int r0 = blockIdx.y * R, r1 = min(B, r0 + R);
+    float s = 0.0f;
+    if (c < N)
+        for (int r = r0 + threadIdx.y; r < r1; r += 8) s += __bfloat162float(D[(size_t)r * N + c]);
+    acc[threadIdx.y][threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.y == 0 && c < N) {
+        float t = acc[0][threadIdx.x];
+        for (int k = 1; k < 8; ++k) t += acc[k][threadIdx.x];
+        part[(size_t)blockIdx.y * N + c] = t;
+    }
+}
+
+__global__ void k_colsum_final(const float* __restrict__ part, int N, int n_valid, float* __restrict__ out) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= n_valid) return;
     float s = 0.0f;
-    for (int r = 0; r < B; ++r) s += __bfloat162float(D[(size_t)r * N + c]);
+    for (int k = 0; k < kColChunks; ++k) s += part[(size_t)k * N + c];
     out[c] = s;
+}
+
+// acc[0] += sum of the loss partials (one thread, fixed order).
+__global__ void k_loss_accumulate(const double* __restrict__ part, int n, double* __restrict__ acc) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += part[i];
+    acc[0] += s;
 }
 
 __global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m1,
@@ -152,6 +181,8 @@ struct ms_mlp {
     __nv_bfloat16 *dZ = nullptr, *dZ2 = nullptr, *dZT = nullptr;
     float *Y = nullptr, *Tb = nullptr, *part = nullptr;
     double* loss_part = nullptr;
+    double* loss_acc = nullptr;   // [1] running sum over an epoch
+    float* colpart = nullptr;     // [kColChunks][width] bias-gradient partials
     size_t part_cap = 0;
     int* err = nullptr;
     // data set
@@ -244,6 +275,8 @@ ms_status ensure_batch(ms_mlp* h, int rows) {
     ML_TRY(malloc_dev(h, &h->Y, (size_t)B * 16));
     ML_TRY(malloc_dev(h, &h->Tb, (size_t)B * h->out_dim));
     ML_TRY(malloc_dev(h, &h->loss_part, 1024));
+    ML_TRY(malloc_dev(h, &h->loss_acc, 1));
+    ML_TRY(malloc_dev(h, &h->colpart, (size_t)kColChunks * std::max(h->width, 16)));
     h->cap = rows;
     return MS_OK;
 }
@@ -338,7 +371,9 @@ ms_status backward(ms_mlp* h, int B) {
         ML_CUDA(h, gemm(a, tc::EPI_F32, S, h->stream));
         const int nw = y.N * Kin;
         k_splitk_sum<<<(nw + 255) / 256, 256, 0, h->stream>>>(h->part, S, Mp, Kin, y.N, Kin, h->g + y.w_off);
-        k_colsum<<<(y.N + 127) / 128, 128, 0, h->stream>>>(dZcur, B, y.Np, y.N, h->g + y.b_off);
+        k_colsum_part<<<dim3((y.Np + 31) / 32, kColChunks), dim3(32, 8), 0, h->stream>>>(dZcur, B, y.Np,
+                                                                                         h->colpart);
+        k_colsum_final<<<(y.N + 127) / 128, 128, 0, h->stream>>>(h->colpart, y.Np, y.N, h->g + y.b_off);
         ML_CUDA(h, cudaGetLastError());
         if (l == 0) break;
         // dZ_{l-1} = (dZ_l W_l) * SiLU'(Z_{l-1})
@@ -586,12 +621,11 @@ ms_status ms_mlp_train(ms_mlp* h, int32_t epochs, int32_t batch, double lr, uint
     std::vector<long long> perm(n);
     std::mt19937_64 rng(seed);
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-    std::vector<double> part(256);
     for (int ep = 0; ep < epochs; ++ep) {
         for (long long i = 0; i < n; ++i) perm[i] = i;
         std::shuffle(perm.begin(), perm.end(), rng);
         ML_CUDA(h, cudaMemcpyAsync(h->d_idx, perm.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, h->stream));
-        double ep_sum = 0.0;
+        ML_CUDA(h, cudaMemsetAsync(h->loss_acc, 0, sizeof(double), h->stream));
         for (long long r0 = 0; r0 < n; r0 += B) {
             const int rows = (int)std::min<long long>(B, n - r0);
             k_gather<<<B, 64, 0, h->stream>>>(h->dX, h->dT, h->d_idx, r0, n, h->in_dim, h->in_pad, h->out_dim, B,
@@ -605,13 +639,11 @@ ms_status ms_mlp_train(ms_mlp* h, int32_t epochs, int32_t batch, double lr, uint
                                                                                 (long long)h->n_params, (float)lr,
                                                                                 b1, b2, eps, c1, c2);
             ML_TRY(refresh_bf16(h));
-            ML_CUDA(h, cudaMemcpyAsync(part.data(), h->loss_part, 256 * sizeof(double), cudaMemcpyDeviceToHost,
-                                       h->stream));
-            ML_CUDA(h, cudaStreamSynchronize(h->stream));
-            double s = 0.0;
-            for (double v : part) s += v;
-            ep_sum += s;
+            k_loss_accumulate<<<1, 1, 0, h->stream>>>(h->loss_part, 256, h->loss_acc);
         }
+        double ep_sum = 0.0;
+        ML_CUDA(h, cudaMemcpyAsync(&ep_sum, h->loss_acc, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        ML_CUDA(h, cudaStreamSynchronize(h->stream));
         ML_TRY(check_err(h));
         if (epoch_loss) epoch_loss[ep] = (float)(ep_sum / ((double)n * h->out_dim));
     }

@@ -156,8 +156,11 @@ __device__ __forceinline__ void node_finish(const DevMesh& m, const DevState& s,
 }
 
 // Entries whose indices, then contributions, one thread loads together.
+#ifndef MSB_NODE_PREFETCH
+#define MSB_NODE_PREFETCH 1
+#endif
 #ifndef MSB_NODE_BATCH
-#define MSB_NODE_BATCH 4
+#define MSB_NODE_BATCH 3
 #endif
 constexpr int kNodeBatch = MSB_NODE_BATCH;
 
@@ -173,10 +176,26 @@ __device__ __forceinline__ void gather_sell(const DevMesh& m, const Cf* __restri
     const int base = __ldg(m.sell_off + w);
     const int width = (__ldg(m.sell_off + w + 1) - base) >> 5;
     const int* __restrict__ ep = m.sell_ent + base + lane;
+#if MSB_NODE_PREFETCH
+    // The next batch's entry ids load together with this batch's
+    // contributions, so each batch costs one round trip, not two.
+    int nx[kNodeBatch];
+#pragma unroll
+    for (int j = 0; j < kNodeBatch; ++j) nx[j] = (j < width) ? __ldg(ep + 32 * j) : -1;
+#endif
     for (int k = 0; k < width; k += kNodeBatch) {
         int ei[kNodeBatch];
+#if MSB_NODE_PREFETCH
+#pragma unroll
+        for (int j = 0; j < kNodeBatch; ++j) {
+            ei[j] = nx[j];
+            const int kk = k + kNodeBatch + j;
+            nx[j] = (kk < width) ? __ldg(ep + 32 * kk) : -1;
+        }
+#else
 #pragma unroll
         for (int j = 0; j < kNodeBatch; ++j) ei[j] = (k + j < width) ? __ldg(ep + 32 * (k + j)) : -1;
+#endif
         Cf v[kNodeBatch][3];
         constexpr int S = std::is_same<Cf, float>::value ? kMixedSlot : 3;
 #pragma unroll
