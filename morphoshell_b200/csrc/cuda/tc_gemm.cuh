@@ -9,9 +9,10 @@
 // cp.async copies, in the canonical K-major no-swizzle layout of the MMA's
 // shared-memory descriptors (8-row x 16-byte core matrices: consecutive
 // 8-row groups 128 B apart, the two 16-byte K halves of a K=16 step
-// `rows/8 * 128` B apart); thread 0 issues tcgen05.mma (M = 128, N = BN,
-// K = 16) four times per stage and commits them to the stage's mbarrier,
-// so the next stage loads while the tensor cores work; the epilogue reads
+// `rows/8 * 128` B apart), kStages stages deep: while the tensor cores work
+// on one stage the next two are in flight.  Thread 0 issues tcgen05.mma
+// (M = 128, N = BN, K = 16) four times per stage and commits them to the
+// stage's mbarrier, which frees the stage for its refill; the epilogue reads
 // the accumulator with tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 =
 // rows) and applies a fused bias / activation.  Every mbarrier wait is
 // bounded: on timeout the kernel records an error and still frees its
@@ -29,6 +30,7 @@ namespace tc {
 constexpr int kBM = 128;
 constexpr int kBK = 64;
 constexpr int kThreads = 128;
+constexpr int kStages = 3;  // shared-memory stages of the K loop
 
 enum Epilogue {
     EPI_F32 = 0,        // Cf = acc (+ bias[n])
@@ -163,7 +165,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
     constexpr int kABytes = kBM * kBK * 2, kBBytes = BN * kBK * 2;
     constexpr int kStage = kABytes + kBBytes;
     constexpr uint32_t kCols = BN < 32 ? 32 : BN;  // TMEM columns (power of two >= 32)
-    __shared__ uint64_t bar[2];
+    __shared__ uint64_t bar[kStages];
     __shared__ uint32_t tmem_slot;
     __shared__ int failed;
 
@@ -172,8 +174,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
     const int kb = blockIdx.z * g.k_split, ke = min(g.K, kb + g.k_split);
 
     if (threadIdx.x == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int i = 0; i < kStages; ++i) mbar_init(&bar[i], 1);
         failed = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -189,28 +190,37 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
     const uint32_t tmem = tmem_slot;
     const uint32_t idesc = instr_desc_bf16(BN);
     const uint32_t base = smem_u32(smem);
-
-    uint32_t phase[2] = {0u, 0u};
     const int nk = (ke - kb + kBK - 1) / kBK;
-    for (int kt = 0; kt < nk; ++kt) {
-        const int s = kt & 1;
-        if (kt >= 2) {  // the MMAs of step kt-2 read this stage
-            if (!mbar_wait_bounded(&bar[s], phase[s])) failed = 1;
-            phase[s] ^= 1u;
-        }
-        __syncthreads();
-        if (failed) break;  // uniform after the barrier
+
+    // K step kt lives in slot kt % kStages; the j-th commit to a slot's
+    // mbarrier is step kStages j + slot, so step kt's MMAs are done when the
+    // phase of parity (kt / kStages) & 1 of bar[kt % kStages] completes.
+    auto load = [&](int kt) {
+        const int s = kt % kStages;
         const int k0 = kb + kt * kBK;
         const int kv = min(kBK, ke - k0);
         const uint32_t sa = base + s * kStage, sb = sa + kABytes;
         stage_tile<kBM>(sa, g.A + (size_t)m0 * g.lda + k0, g.lda, kv, smem + s * kStage);
         stage_tile<BN>(sb, g.B + (size_t)n0 * g.ldb + k0, g.ldb, kv, smem + s * kStage + kABytes);
+    };
+    // Prologue: steps 0 .. kStages-2 in flight (one copy group each, empty
+    // groups past the end keep the count uniform).
+#pragma unroll
+    for (int p = 0; p < kStages - 1; ++p) {
+        if (p < nk) load(p);
         asm volatile("cp.async.commit_group;" ::: "memory");
-        asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    int last = -1;  // last step whose MMAs were committed
+    for (int kt = 0; kt < nk; ++kt) {
+        const int s = kt % kStages;
+        // kStages-1+kt groups committed; step kt's is the (kStages-2)-th newest.
+        asm volatile("cp.async.wait_group %0;" ::"n"(kStages - 2) : "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (threadIdx.x == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int kv = min(kBK, ke - (kb + kt * kBK));
+            const uint32_t sa = base + s * kStage, sb = sa + kABytes;
 #pragma unroll
             for (int j = 0; j < kBK / 16; ++j) {
                 if (j * 16 < kv) {
@@ -221,18 +231,27 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
             }
             mma_commit(&bar[s]);
         }
+        last = kt;
+        // Refill: step kt+kStages-1 goes into the slot step kt-1 used, once
+        // that step's MMAs are done (step kt's are already queued behind).
+        const int nxt = kt + kStages - 1;
+        if (nxt < nk) {
+            int ok = 1;
+            if (kt >= 1) ok = mbar_wait_bounded(&bar[(kt - 1) % kStages], ((kt - 1) / kStages) & 1) ? 1 : 0;
+            if (!__syncthreads_and(ok)) {
+                if (threadIdx.x == 0) failed = 1;
+                break;
+            }
+            load(nxt);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
     }
-    // The last commit covers every earlier MMA.
-    if (!failed && nk > 0) {
-        const int s = (nk - 1) & 1;
-        if (!mbar_wait_bounded(&bar[s], phase[s])) failed = 1;
-    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncthreads();
-    if (failed && threadIdx.x == 0) {
-        // Give MMAs still in flight a bounded chance to finish before the
-        // tensor memory is freed.
-        mbar_wait_bounded(&bar[0], phase[0]);
-        mbar_wait_bounded(&bar[1], phase[1]);
+    // The last commit covers every earlier MMA.
+    if (last >= 0) {
+        const bool ok = mbar_wait_bounded(&bar[last % kStages], (last / kStages) & 1);
+        if (!ok && threadIdx.x == 0) failed = 1;
     }
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -298,7 +317,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(const GemmArgs g) {
 
 template <int BN>
 constexpr int gemm_smem_bytes() {
-    return 2 * (kBM * kBK * 2 + BN * kBK * 2);
+    return kStages * (kBM * kBK * 2 + BN * kBK * 2);
 }
 
 }  // namespace tc
