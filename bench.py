@@ -139,15 +139,16 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(workload: str, precision: str):
-    """DRAM bytes per step from the committed ncu summary, if one exists."""
+def profiled_traffic(workload: str, precision: str, path: str):
+    """DRAM bytes per step from the committed ncu summary, if one exists
+    (lines ``workload precision path bytes``)."""
     p = os.path.join(ROOT, "profiles", "step_traffic.txt")
     try:
         with open(p) as f:
             for line in f:
-                parts = line.split()
-                if len(parts) >= 3 and parts[0] == workload and parts[1] == precision:
-                    return float(parts[2])
+                parts = line.split("#")[0].split()
+                if len(parts) >= 4 and parts[:3] == [workload, precision, path]:
+                    return float(parts[3])
     except OSError:
         pass
     return None
@@ -259,7 +260,7 @@ def run_ours(args):
     T = model.num_tris
     prec = MS_PRECISION_MIXED if args.precision == "mixed" else MS_PRECISION_FP64
     g = GpuLoop(model, precision=prec, device=local)
-    g.set_step_path({"cluster": 0, "two-kernel": 1, "tiles": 2}[args.path])
+    g.set_step_path({"cluster": 0, "two-kernel": 1, "tiles": 2, "node-tiles": 3}[args.path])
     plan = g.plan_info()
     g.set_programmed(3, info, bbar, s.dial_factors_to_hold_at_spacing)
     g.upload(model.dofs(1))
@@ -293,7 +294,7 @@ def run_ours(args):
     bpt = BYTES_PER_TRI[args.precision]
     achieved = bpt * T / (step_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
-    traffic = profiled_traffic(args.workload, args.precision)
+    traffic = profiled_traffic(args.workload, args.precision, args.path)
 
     # End to end through the C ABI with the state on the host every step.
     N = model.num_nodes
@@ -329,18 +330,20 @@ def run_ours(args):
 
     clocks = clk.summary()
     tri_name, node_name = {"cluster": ("k_cluster_step", "k_halo_update"), "two-kernel": ("k_tri_aos", "k_node_update"),
-                           "tiles": ("k_tri_tiles", "k_node_update")}[args.path]
+                           "tiles": ("k_tri_tiles", "k_node_update"), "node-tiles": ("k_node_tiles", None)}[args.path]
+    kernels_per_step = 1 if node_name is None else 2
+    kernel_ms = {tri_name: t_tri} if node_name is None else {tri_name: t_tri, node_name: t_node}
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed", "data": "synthetic",
         "config": workload_config(args, model),
-        "gpu_launches": 2 * args.steps + (args.steps + 127) // 128,
+        "gpu_launches": kernels_per_step * args.steps + (args.steps + 127) // 128,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "one step = %s + %s" % (tri_name, node_name),
+                     "kernel": "one step = " + " + ".join(k for k in (tri_name, node_name) if k),
                      "algorithmic_bytes_per_tri": bpt,
-                     "kernel_ms": {tri_name: t_tri, node_name: t_node}},
+                     "kernel_ms": kernel_ms},
         "plan": plan,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 2 * 24 * N + 8,
                 "d2h_bytes_per_step": 2 * 24 * N + 16, "steps": e2e_steps},
@@ -505,7 +508,7 @@ def main():
     ap.add_argument("--workload", default="disk1p8m")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
-    ap.add_argument("--path", choices=["cluster", "two-kernel", "tiles"], default="tiles",
+    ap.add_argument("--path", choices=["cluster", "two-kernel", "tiles", "node-tiles"], default="tiles",
                     help="fused-step implementation (ms_set_step_path)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

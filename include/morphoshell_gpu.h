@@ -206,9 +206,12 @@ void* ms_stream(ms_handle* h);
  * interior nodes itself; 1 the two-kernel step (per-triangle kernel writes
  * all contributions to HBM, per-node kernel gathers them); 2 (default) the
  * two-kernel step whose per-triangle kernel is persistent and streams its
- * tables through shared memory with bulk asynchronous copies.  All sum
- * every node's contributions in ascending triangle order, so they give the
- * same bits. */
+ * tables through shared memory with bulk asynchronous copies; 3 the
+ * node-tiled step -- one kernel: each block takes tiles of consecutive
+ * nodes, computes every triangle that touches the tile (border triangles
+ * once per tile), sums the tile's forces in shared memory and updates its
+ * nodes, so no contribution goes through HBM.  All sum every node's
+ * contributions in ascending triangle order, so they give the same bits. */
 ms_status ms_set_step_path(ms_handle* h, int path);
 /* Tiling of the cluster path: CTAs per cluster, triangles per CTA, number of
  * clusters, number of halo nodes (summed by the second kernel), and the
@@ -216,9 +219,30 @@ ms_status ms_set_step_path(ms_handle* h, int path);
 ms_status ms_plan_info(ms_handle* h, int* cluster_size, int* tris_per_cta, int* clusters, int* halo_nodes,
                        int* path);
 
+/* Layout of the node-tiled step (path 3) for a mesh and a tile size, computed
+ * on the host alone (no device needed), with the same code and the same
+ * bounds checks ms_create runs: node tiles, chunk records (128 triangle
+ * slots each), triangles computed per step (a border triangle once per tile
+ * it touches), the largest node section and the record stride in bytes,
+ * the record bytes copied per step and the shared memory a block needs.
+ * Returns MS_ERR_INVALID_ARGUMENT for bad arguments or lists that fail the
+ * checks. */
+typedef struct ms_node_tile_info {
+    int tiles;
+    int chunks;
+    long long tri_tile_pairs;
+    long long node_section_max;
+    long long record_stride;
+    long long bytes_per_step;
+    long long shared_bytes;
+} ms_node_tile_info;
+ms_status ms_node_tile_layout(int num_nodes, int num_tris, const int* patch_ids, int nodes_per_tile, int precision,
+                              ms_node_tile_info* out);
+
 /* Mean device time of one launch of each fused-step kernel over `reps`
  * steps (CUDA events on the handle's stream; the steps advance the state):
- * the per-triangle kernel (ms_tri) and the per-node kernel (ms_node). */
+ * the per-triangle kernel (ms_tri) and the per-node kernel (ms_node); on
+ * the node-tiled path the one kernel is ms_tri and ms_node is 0. */
 ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial_factor, double timestep,
                           double damping_factor, double* ms_tri, double* ms_node);
 

@@ -27,7 +27,7 @@ GPU_SYMBOLS = [
     "ms_download_programmed", "ms_surface_derivs", "ms_a_b_normals", "ms_deformation_forces",
     "ms_non_deformation_forces", "ms_impose_constraints", "ms_is_at_equilibrium", "ms_advance_dynamics",
     "ms_step_n", "ms_output_quantities", "ms_device_info", "ms_stream", "ms_time_kernels",
-    "ms_deformation_forces_noalloc", "ms_set_step_path", "ms_plan_info",
+    "ms_deformation_forces_noalloc", "ms_set_step_path", "ms_plan_info", "ms_node_tile_layout",
     "ms_batch_create", "ms_batch_destroy", "ms_batch_last_error", "ms_batch_run", "ms_batch_status",
     "ms_batch_download_dofs", "ms_batch_upload_dofs", "ms_batch_set_schedule", "ms_batch_get_schedule",
     "ms_batch_autotune", "ms_batch_info", "ms_batch_stream", "ms_batch_set_start",
@@ -97,6 +97,12 @@ class msh_run_result(C.Structure):
                 ("last_max_speed_ratio", C.c_double)]
 
 
+class ms_node_tile_info(C.Structure):
+    _fields_ = [("tiles", C.c_int), ("chunks", C.c_int), ("tri_tile_pairs", C.c_longlong),
+                ("node_section_max", C.c_longlong), ("record_stride", C.c_longlong),
+                ("bytes_per_step", C.c_longlong), ("shared_bytes", C.c_longlong)]
+
+
 class ms_batch_instance(C.Structure):
     _fields_ = [("mesh", ms_mesh_desc), ("params", ms_params), ("abar_info", C.POINTER(C.c_double)),
                 ("timestep", C.c_double), ("damping_factor_1", C.c_double), ("damping_factor_2", C.c_double),
@@ -162,6 +168,7 @@ def lib() -> C.CDLL:
         L.ms_set_step_path.argtypes = [C.c_void_p, C.c_int]
         ip = C.POINTER(C.c_int)
         L.ms_plan_info.argtypes = [C.c_void_p, ip, ip, ip, ip, ip]
+        L.ms_node_tile_layout.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, P(ms_node_tile_info)]
         L.ms_stream.argtypes = [C.c_void_p]
         L.ms_stream.restype = C.c_void_p
         L.ms_time_kernels.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, d, d]
@@ -431,8 +438,9 @@ class GpuLoop:
         return rep
 
     def set_step_path(self, path: int):
-        """0: cluster-tiled step, 1: two-kernel step, 2 (default): two-kernel
-        step with the per-triangle tables fed by bulk asynchronous copies."""
+        """0: cluster-tiled step, 1: two-kernel step, 2: two-kernel step with
+        the per-triangle tables fed by bulk asynchronous copies, 3: node-tiled
+        one-kernel step (forces summed in shared memory per tile of nodes)."""
         self._chk(lib().ms_set_step_path(self._h, path), "set_step_path")
 
     def plan_info(self) -> dict:
@@ -666,6 +674,21 @@ def run_batch(models, max_steps: int = 0, precision: int = MS_PRECISION_FP64, de
     if rc != 0:
         raise RuntimeError(lib().msh_last_error().decode())
     return [(res[i], outs[i]) for i in range(n)]
+
+
+def node_tile_layout(patch_ids, num_nodes: int, nodes_per_tile: int = 1024,
+                     precision: int = MS_PRECISION_FP64) -> dict:
+    """Layout of the node-tiled step (step path 3) for a mesh's patch table
+    ([T][6] node ids), computed on the host with the checks ms_create runs:
+    tiles, chunks, triangles computed per step, record sizes, shared memory
+    per block."""
+    p = np.ascontiguousarray(patch_ids, dtype=np.int32)
+    info = ms_node_tile_info()
+    rc = lib().ms_node_tile_layout(int(num_nodes), p.shape[0], p.ctypes.data, int(nodes_per_tile), int(precision),
+                                   C.byref(info))
+    if rc != 0:
+        raise MsError(rc, "ms_node_tile_layout failed")
+    return {k: getattr(info, k) for k, _ in ms_node_tile_info._fields_}
 
 
 def device_info() -> str:

@@ -79,6 +79,11 @@ struct ms_handle {
     bool have_tiles = false;
     unsigned char* d_tiles = nullptr;
     size_t tile_bytes = 0;
+    // node-tiled step
+    bool have_ntiles = false;
+    NodeTilePlan ntp{};
+    unsigned char* d_nt_rec = nullptr;
+    std::vector<int> nt_chunk_tri;  // host copy of NodeTilePlan::chunk_tri
 };
 
 namespace {
@@ -222,6 +227,220 @@ ms_status build_tiles(ms_handle* h, const ms_mesh_desc* d) {
     return MS_OK;
 }
 
+#ifndef MSB_NT_NODES
+#define MSB_NT_NODES 1024
+#endif
+
+// Host-side layout of the node-tiled step (NodeTilePlan) for tiles of NT
+// consecutive nodes: every tile's triangle list (ascending t), its chunks and
+// their node sections, checked against the bounds the kernel relies on.
+struct NodeTileLayout {
+    int K = 0, C = 0;
+    std::vector<long long> start;   // [K + 1] list offsets into lst
+    std::vector<int> lst;           // triangle lists, tile after tile
+    std::vector<int> tile_chunk;    // [K + 1]
+    std::vector<std::vector<unsigned short>> run_node, run_end, cent;  // per chunk
+    std::vector<unsigned> bytes;    // [C] bytes to copy (fixed part + node section)
+    size_t fixed = 0, stride = 0, ns_max = 0;
+};
+
+bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, const std::vector<int>& off,
+                      const std::vector<int>& ent, NodeTileLayout& L, std::string& err) {
+    if (NT <= 0 || NT > 65536) {
+        err = "nodes per tile must be in 1..65536";
+        return false;
+    }
+    const int K = (N + NT - 1) / NT;
+    L.K = K;
+    L.start.assign(K + 1, 0);
+    auto tiles_of = [&](int t, int* out) {
+        int n = 0;
+        for (int k = 0; k < 6; ++k) {
+            const int tk = patch_ids[6LL * t + k] / NT;
+            bool seen = false;
+            for (int j = 0; j < n; ++j) seen = seen || out[j] == tk;
+            if (!seen) out[n++] = tk;
+        }
+        return n;
+    };
+    int tk[6];
+    for (int t = 0; t < T; ++t) {
+        const int n = tiles_of(t, tk);
+        for (int j = 0; j < n; ++j) L.start[tk[j] + 1] += 1;
+    }
+    for (int k = 0; k < K; ++k) L.start[k + 1] += L.start[k];
+    L.lst.assign(L.start[K], 0);
+    {
+        std::vector<long long> fill(L.start.begin(), L.start.end() - 1);
+        for (int t = 0; t < T; ++t) {
+            const int n = tiles_of(t, tk);
+            for (int j = 0; j < n; ++j) L.lst[fill[tk[j]]++] = t;
+        }
+    }
+    L.tile_chunk.assign(K + 1, 0);
+    // At least one chunk per tile (an empty one for a tile of isolated
+    // nodes), so that every tile's walk starts with a copy of its own record.
+    for (int k = 0; k < K; ++k)
+        L.tile_chunk[k + 1] =
+            L.tile_chunk[k] + std::max(1, (int)((L.start[k + 1] - L.start[k] + kTile - 1) / kTile));
+    const int C = L.tile_chunk[K];
+    L.C = C;
+    // Node sections: for each chunk, runs (node in tile, end) and entries
+    // (slot * 6 + patch slot).  Nodes go in ascending order and each node's
+    // entries in ascending t, so a node's entries within a chunk are one run.
+    L.run_node.assign(C, {});
+    L.run_end.assign(C, {});
+    L.cent.assign(C, {});
+    std::vector<int> run_last(C, -1);
+    for (int k = 0; k < K; ++k) {
+        const int* L0 = L.lst.data() + L.start[k];
+        const int* L1 = L.lst.data() + L.start[k + 1];
+        for (int n = k * NT; n < std::min(N, (k + 1) * NT); ++n) {
+            int last_t = -1;
+            for (int e = off[n]; e < off[n + 1]; ++e) {
+                const int t = ent[e] / 6, slot = ent[e] % 6;
+                const int li = (int)(std::lower_bound(L0, L1, t) - L0);
+                if (L0 + li == L1 || L0[li] != t || t < last_t) {
+                    err = "incidence lists disagree with the patches";
+                    return false;
+                }
+                last_t = t;
+                const int c = L.tile_chunk[k] + li / kTile;
+                const int j = n - k * NT;
+                if (run_last[c] != j) {
+                    L.run_node[c].push_back((unsigned short)j);
+                    L.run_end[c].push_back(L.run_end[c].empty() ? 0 : L.run_end[c].back());
+                    run_last[c] = j;
+                }
+                L.cent[c].push_back((unsigned short)((li % kTile) * 6 + slot));
+                L.run_end[c].back() += 1;
+            }
+        }
+    }
+    L.fixed = tile_record_bytes(mixed);
+    L.ns_max = 16;
+    L.bytes.assign(C, 0);
+    for (int k = 0; k < K; ++k) {
+        for (int c = L.tile_chunk[k]; c < L.tile_chunk[k + 1]; ++c) {
+            const long long first = L.start[k] + (long long)(c - L.tile_chunk[k]) * kTile;
+            const int ntri = (int)std::max<long long>(0, std::min<long long>(kTile, L.start[k + 1] - first));
+            const size_t R = L.run_node[c].size(), E = L.cent[c].size();
+            // What the kernel indexes: entries inside the chunk's live slots,
+            // run nodes inside the tile's accumulators, run ends ascending up
+            // to E, everything inside one record.
+            bool ok = R <= 6 * kTile && E <= 6 * kTile;
+            for (size_t r = 0; ok && r < R; ++r)
+                ok = L.run_node[c][r] < NT && L.run_end[c][r] > (r ? L.run_end[c][r - 1] : 0);
+            ok = ok && (R == 0 ? E == 0 : L.run_end[c][R - 1] == E);
+            for (size_t e = 0; ok && e < E; ++e) ok = L.cent[c][e] < 6 * ntri;
+            if (!ok) {
+                err = "node tile chunk fails its bounds";
+                return false;
+            }
+            const size_t ns = (16 + 4 * R + 2 * E + 15) / 16 * 16;
+            L.ns_max = std::max(L.ns_max, ns);
+            L.bytes[c] = (unsigned)(L.fixed + ns);
+        }
+    }
+    L.stride = L.fixed + (L.ns_max + 127) / 128 * 128;
+    return true;
+}
+
+#ifndef MSB_NT_NODES
+#define MSB_NT_NODES 1024
+#endif
+
+// Plan of the node-tiled step for tiles of MSB_NT_NODES nodes: the chunk
+// records, area in the trigonometry block (cos^2 = 1, the rest 0) until
+// prepare_lce_tables writes the director's values.  Leaves the other paths in
+// place when the kernel cannot be set up.
+ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vector<int>& off,
+                           const std::vector<int>& ent) {
+    const int N = d->num_nodes, T = d->num_tris, NT = MSB_NT_NODES;
+    const int mixed = h->precision == MS_PRECISION_MIXED;
+    if (N <= 0 || T <= 0) return MS_OK;
+    NodeTileLayout L;
+    std::string err;
+    if (!node_tile_layout(d->patch_ids, N, T, NT, mixed, off, ent, L, err)) return fail(h, MS_ERR_INVALID_ARGUMENT, err);
+    const int K = L.K, C = L.C;
+    const size_t stride = L.stride, fixed = L.fixed;
+    const size_t smem = node_tile_smem(stride, NT);
+    int blocks = 0;
+    if (smem > 227 * 1024 || prepare_node_tile_kernels(mixed, smem, &blocks) != cudaSuccess || blocks <= 0) {
+        cudaGetLastError();
+        h->have_ntiles = false;
+        return MS_OK;  // the other paths remain
+    }
+    std::vector<unsigned char> buf(stride * C, 0);
+    std::vector<int>& ctri = h->nt_chunk_tri;
+    ctri.assign((size_t)C * kTile, -1);
+    const size_t ids_b = 6 * kTile * 4, coef_b = 24 * kTile * (mixed ? 4 : 8);
+    for (int k = 0; k < K; ++k) {
+        for (int c = L.tile_chunk[k]; c < L.tile_chunk[k + 1]; ++c) {
+            unsigned char* r = buf.data() + stride * c;
+            int32_t* ids = reinterpret_cast<int32_t*>(r);
+            double* aux = reinterpret_cast<double*>(r + ids_b + coef_b);
+            const long long first = L.start[k] + (long long)(c - L.tile_chunk[k]) * kTile;
+            const int ntri = (int)std::max<long long>(0, std::min<long long>(kTile, L.start[k + 1] - first));
+            for (int i = 0; i < ntri; ++i) {
+                const int t = L.lst[first + i];
+                ctri[(size_t)c * kTile + i] = t;
+                for (int q = 0; q < 6; ++q) ids[q * kTile + i] = d->patch_ids[6LL * t + q];
+                const double* w = d->deriv_coeffs + 24LL * t;
+                if (mixed) {
+                    float* cf = reinterpret_cast<float*>(r + ids_b);
+                    for (int q = 0; q < 24; ++q) cf[q * kTile + i] = (float)w[q];
+                } else {
+                    double* cf = reinterpret_cast<double*>(r + ids_b);
+                    for (int q = 0; q < 24; ++q) cf[q * kTile + i] = w[q];
+                }
+                aux[i] = d->ref_area[t];
+                aux[kTile + i] = 1.0;
+            }
+            int32_t* hd = reinterpret_cast<int32_t*>(r + fixed);
+            const int R = (int)L.run_node[c].size(), E = (int)L.cent[c].size();
+            hd[0] = R;
+            hd[1] = E;
+            hd[2] = ntri;
+            unsigned short* u = reinterpret_cast<unsigned short*>(r + fixed + 16);
+            std::copy(L.run_node[c].begin(), L.run_node[c].end(), u);
+            std::copy(L.run_end[c].begin(), L.run_end[c].end(), u + R);
+            std::copy(L.cent[c].begin(), L.cent[c].end(), u + 2 * R);
+        }
+    }
+    unsigned char* d_rec;
+    int *d_tile_chunk, *d_ctri;
+    unsigned* d_bytes;
+    MS_TRY(upload(h, &d_rec, buf));
+    MS_TRY(upload(h, &d_tile_chunk, L.tile_chunk));
+    MS_TRY(upload(h, &d_bytes, L.bytes));
+    MS_TRY(upload(h, &d_ctri, ctri));
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    NodeTilePlan& q = h->ntp;
+    q.nodes = NT;
+    q.ntiles = K;
+    q.nchunks = C;
+    q.grid = sms * blocks;
+    q.stride = stride;
+    q.rec = d_rec;
+    q.tile_chunk = d_tile_chunk;
+    q.chunk_bytes = d_bytes;
+    q.chunk_tri = d_ctri;
+    h->d_nt_rec = d_rec;
+    // One equilibrium partial per block.
+    const int parts = std::min(K, q.grid);
+    if (parts > h->s.eq_blocks) {
+        EqPartial* ep;
+        MS_TRY(dalloc(h, &ep, parts));
+        h->s.eq_part = ep;
+        h->s.eq_blocks = parts;
+    }
+    h->have_ntiles = true;
+    return MS_OK;
+}
+
 // Tiles of cs * tpc consecutive triangles, one per thread-block cluster; a
 // node is owned by a tile when all its incidences lie in it (see
 // ClusterPlan).  Falls back to the two-kernel step when cluster launches are
@@ -313,7 +532,8 @@ ms_status build_cluster_plan(ms_handle* h, const ms_mesh_desc* d, const std::vec
         h->s.eq_blocks = parts;
     }
     h->have_plan = true;
-    return build_tiles(h, d);
+    MS_TRY(build_tiles(h, d));
+    return build_node_tiles(h, d, off, ent);
 }
 
 // Per-triangle director trigonometry for the cluster kernel's protocol-3
@@ -353,6 +573,19 @@ ms_status prepare_lce_tables(ms_handle* h, const double* info, int ka) {
         const size_t off = 6 * kTile * 4 + 24 * kTile * (h->precision == MS_PRECISION_MIXED ? 4 : 8);
         MS_CUDA(h, cudaMemcpy2D(h->d_tiles + off, h->tile_bytes, blk.data(), 4 * kTile * sizeof(double),
                                 4 * kTile * sizeof(double), ntiles, cudaMemcpyHostToDevice));
+    }
+    if (h->have_ntiles) {
+        const int C = h->ntp.nchunks;
+        std::vector<double> blk(4ULL * kTile * C, 0.0);
+        for (size_t j = 0; j < h->nt_chunk_tri.size(); ++j) {
+            const int t = h->nt_chunk_tri[j];
+            if (t < 0) continue;
+            const size_t c = j / kTile, i = j % kTile;
+            for (int k = 0; k < 4; ++k) blk[c * 4 * kTile + k * kTile + i] = aux[4ULL * t + k];
+        }
+        const size_t off = 6 * kTile * 4 + 24 * kTile * (h->precision == MS_PRECISION_MIXED ? 4 : 8);
+        MS_CUDA(h, cudaMemcpy2D(h->d_nt_rec + off, h->ntp.stride, blk.data(), 4 * kTile * sizeof(double),
+                                4 * kTile * sizeof(double), C, cudaMemcpyHostToDevice));
     }
     h->plan.lce_uniform = uniform ? 1 : 0;
     h->lce_lam_final = ln[0];
@@ -794,6 +1027,8 @@ static cudaError_t launch_step(ms_handle* h, const StepScalars& sc, bool cluster
     if (cluster) {
         e = launch_cluster_step(h->m, h->plan, h->s, sc, dial_mode, h->precision, st);
         if (e == cudaSuccess) e = launch_halo_update(h->m, h->plan, h->s, sc, h->precision, st);
+    } else if (h->step_path == 3 && h->have_ntiles) {
+        e = launch_node_tiles(h->m, h->plan, h->ntp, h->s, sc, dial_mode, h->precision, st);
     } else {
         if (h->step_path == 2 && h->have_tiles)
             e = launch_tri_tiles(h->m, h->plan, h->s, sc, dial_mode, h->precision, st);
@@ -805,9 +1040,10 @@ static cudaError_t launch_step(ms_handle* h, const StepScalars& sc, bool cluster
 }
 
 ms_status ms_set_step_path(ms_handle* h, int path) {
-    if (!h || path < 0 || path > 2) return MS_ERR_INVALID_ARGUMENT;
+    if (!h || path < 0 || path > 3) return MS_ERR_INVALID_ARGUMENT;
     if (path == 0 && !h->have_cluster) return fail(h, MS_ERR_UNSUPPORTED, "cluster launches are unavailable");
     if (path == 2 && !h->have_tiles) return fail(h, MS_ERR_UNSUPPORTED, "bulk-copy tile kernel unavailable");
+    if (path == 3 && !h->have_ntiles) return fail(h, MS_ERR_UNSUPPORTED, "node-tiled kernel unavailable");
     h->step_path = path;
     return MS_OK;
 }
@@ -834,7 +1070,7 @@ ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, doub
     while (done < n) {
         const int len = std::min(kChunk, n - done);
         const bool last_chunk = done + len == n;
-        GraphKey key{len, p0 ^ (done & 1), dial_mode + (cluster ? 16 : 0) + (h->step_path == 2 ? 32 : 0), gd,
+        GraphKey key{len, p0 ^ (done & 1), dial_mode + (cluster ? 16 : 0) + (h->step_path == 2 ? 32 : 0) + (h->step_path == 3 ? 64 : 0), gd,
                      (check_last && last_chunk) ? 1 : 0,
                      dt, damping};
         cudaGraphExec_t exec = nullptr;
@@ -949,12 +1185,14 @@ ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial, dou
         const int mode = fuse_lce ? DIAL_LCE : DIAL_ARRAYS;
         MS_CUDA(h, cudaEventRecord(ev[3 * i], st));
         if (cluster) MS_CUDA(h, launch_cluster_step(h->m, h->plan, h->s, sc, mode, h->precision, st));
+        else if (h->step_path == 3 && h->have_ntiles)
+            MS_CUDA(h, launch_node_tiles(h->m, h->plan, h->ntp, h->s, sc, mode, h->precision, st));
         else if (h->step_path == 2 && h->have_tiles)
             MS_CUDA(h, launch_tri_tiles(h->m, h->plan, h->s, sc, mode, h->precision, st));
         else MS_CUDA(h, launch_tri_aos(h->m, h->plan, h->s, sc, mode, h->precision, st));
         MS_CUDA(h, cudaEventRecord(ev[3 * i + 1], st));
         if (cluster) MS_CUDA(h, launch_halo_update(h->m, h->plan, h->s, sc, h->precision, st));
-        else MS_CUDA(h, launch_node_update(h->m, h->s, sc, h->precision, st));
+        else if (!(h->step_path == 3 && h->have_ntiles)) MS_CUDA(h, launch_node_update(h->m, h->s, sc, h->precision, st));
         MS_CUDA(h, cudaEventRecord(ev[3 * i + 2], st));
         p ^= 1;
     }
@@ -972,7 +1210,7 @@ ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial, dou
     if (h->h_err->flag) return fail(h, MS_ERR_IMPLAUSIBLE_FORCE, "implausibly_high_force during kernel timing");
     h->cur = p;
     *ms_tri = a / reps;
-    *ms_node = b / reps;
+    *ms_node = (!cluster && h->step_path == 3 && h->have_ntiles) ? 0.0 : b / reps;  // path 3 has no node kernel
     return MS_OK;
 }
 
@@ -984,6 +1222,34 @@ ms_status ms_plan_info(ms_handle* h, int* cluster_size, int* tris_per_cta, int* 
     if (clusters) *clusters = h->have_plan ? h->plan.nclusters : 0;
     if (halo_nodes) *halo_nodes = h->have_plan ? h->plan.n_halo : -1;
     if (path) *path = h->have_plan ? h->step_path : 1;
+    return MS_OK;
+}
+
+ms_status ms_node_tile_layout(int num_nodes, int num_tris, const int* patch_ids, int nodes_per_tile, int precision,
+                              ms_node_tile_info* out) {
+    if (num_nodes <= 0 || num_tris <= 0 || !patch_ids || !out) return MS_ERR_INVALID_ARGUMENT;
+    const int N = num_nodes, T = num_tris;
+    for (long long k = 0; k < 6LL * T; ++k)
+        if (patch_ids[k] < 0 || patch_ids[k] >= N) return MS_ERR_INVALID_ARGUMENT;
+    std::vector<int> off(N + 1, 0), ent(6ULL * T);
+    for (long long k = 0; k < 6LL * T; ++k) off[patch_ids[k] + 1] += 1;
+    for (int n = 0; n < N; ++n) off[n + 1] += off[n];
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (int t = 0; t < T; ++t)
+        for (int k = 0; k < 6; ++k) ent[fill[patch_ids[6LL * t + k]]++] = 6 * t + k;
+    NodeTileLayout L;
+    std::string err;
+    if (!node_tile_layout(patch_ids, N, T, nodes_per_tile, precision == MS_PRECISION_MIXED, off, ent, L, err))
+        return MS_ERR_INVALID_ARGUMENT;
+    out->tiles = L.K;
+    out->chunks = L.C;
+    out->tri_tile_pairs = L.start[L.K];
+    out->node_section_max = (long long)L.ns_max;
+    out->record_stride = (long long)L.stride;
+    long long b = 0;
+    for (unsigned x : L.bytes) b += x;
+    out->bytes_per_step = b;
+    out->shared_bytes = (long long)node_tile_smem(L.stride, nodes_per_tile);
     return MS_OK;
 }
 

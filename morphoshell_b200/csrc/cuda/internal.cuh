@@ -126,6 +126,36 @@ struct ClusterPlan {
 // Triangles per tile of the bulk-copy-fed per-triangle kernel.
 constexpr int kTile = 128;
 
+// Node-tiled step (node_tiles.cu): one kernel per step.  The nodes, in their
+// Morton order, are cut into node tiles of `nodes` consecutive nodes.  The
+// triangles whose patch touches a node tile (every triangle that contributes
+// to one of its nodes, in ascending triangle order) are that tile's list; a
+// triangle near a tile border is on the lists of every tile it touches and is
+// computed once for each.  A list is cut into chunks of kTile triangles, each
+// one record: the tile record of the bulk-copy kernel (ids [6][kTile], weights
+// [24][kTile], area and director trigonometry [4][kTile]) followed by the
+// chunk's node section:
+//   int32 header {R, E, ntri, 0}
+//   uint16 run_node[R]   node (index in the tile) of each run
+//   uint16 run_end[R]    end of the run's entries (exclusive, cumulative)
+//   uint16 ent[E]        (slot in chunk) * 6 + patch slot, per node ascending t
+// A block sums a node's contributions run by run, chunk by chunk, so every
+// node's force is the sum in ascending triangle order, as in the node kernel.
+struct NodeTilePlan {
+    int nodes;                       // nodes per tile
+    int ntiles;
+    int nchunks;
+    int grid;                        // persistent blocks
+    size_t stride;                   // bytes between chunk records
+    const unsigned char* rec;        // [nchunks] records (double weights, or float for mixed)
+    const int* tile_chunk;           // [ntiles + 1] first chunk of each tile
+    const unsigned* chunk_bytes;     // [nchunks] bytes to copy of each record (multiple of 16)
+    const int* chunk_tri;            // [nchunks][kTile] triangle of each slot, -1 past the chunk's end
+};
+// Largest node section a chunk record may carry: header, runs and entries of
+// kTile triangles with all 6 slots on the tile.
+constexpr int kNodeSectionMax = 16 + 4 * 6 * kTile + 2 * 6 * kTile;
+
 // Layout of the per-(triangle, slot) force contributions: x, y, z doubles;
 // for the mixed path x, y, z floats, optionally padded with a zero to 16
 // bytes so that the node kernel loads each with one vector load.
@@ -248,6 +278,12 @@ size_t tile_record_bytes(int mixed);
 cudaError_t prepare_tile_kernels(int mixed, int* blocks_per_sm);
 cudaError_t launch_tri_tiles(const DevMesh& m, const ClusterPlan& p, const DevState& s, const StepScalars& sc,
                              int dial_mode, int mixed, cudaStream_t st);
+// Node-tiled step (node_tiles.cu): shared memory per block for a plan,
+// kernel set-up (dynamic shared memory; resident blocks per SM) and launch.
+size_t node_tile_smem(size_t stride, int nodes);
+cudaError_t prepare_node_tile_kernels(int mixed, size_t smem, int* blocks_per_sm);
+cudaError_t launch_node_tiles(const DevMesh& m, const ClusterPlan& p, const NodeTilePlan& q, const DevState& s,
+                              const StepScalars& sc, int dial_mode, int mixed, cudaStream_t st);
 // Largest cluster size (8, 4, 2, 1) whose clusters fill the most SMs, and the
 // CTA shape used with it.
 int choose_cluster_size(int tpc, int threads, int mixed);

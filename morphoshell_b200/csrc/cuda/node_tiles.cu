@@ -1,0 +1,224 @@
+// Node-tiled step (ms_set_step_path 3): the whole fused step in one kernel,
+// with no per-triangle contributions in HBM.
+//
+// A persistent block walks node tiles (blockIdx.x, then every gridDim.x-th).
+// For each tile it streams the chunk records of the tile's triangle list
+// (every triangle whose patch touches one of the tile's nodes, ascending t):
+// thread 0 copies the next record into the other half of a shared-memory
+// double buffer with one cp.async.bulk (completion counted in bytes on an
+// mbarrier; the next tile's first record follows the current tile's last),
+// while the block computes the current chunk.  Each thread computes one
+// triangle's 18 contributions (the arithmetic of the bulk-copy per-triangle
+// kernel, tile_tri), stages them in the consumed weight area, and then the
+// chunk's runs add them to the tile's per-node accumulators in shared
+// memory: one thread per run, a run being one node's entries in this chunk in
+// ascending triangle order.  Chunks are taken in order, so each node's force
+// is summed in ascending triangle order from zero -- the order, and so the
+// bits, of the node kernel's gather (calc_deformation_forces.cpp:185).  After
+// the tile's last chunk the block finishes its nodes (damping, constraints,
+// guard, equilibrium maxima, symplectic Euler; node_core) and moves on.
+//
+// Cost against the two-kernel step: triangles on tile borders are computed
+// once per tile they touch (16-20 % more triangle work at 1024-node tiles),
+// but the contribution round trip through HBM (144 B per triangle in FP64,
+// 72 B mixed) and the node kernel's incidence lists disappear.
+#include <algorithm>
+#include <climits>
+
+#include "internal.cuh"
+#include "step_common.cuh"
+#include "tile_copy.cuh"
+#include "tri_contrib.cuh"
+
+namespace msb {
+namespace {
+
+using namespace stepdev;
+using namespace tridev;
+using namespace tiles;
+
+// Nodes finished per thread with their loads in flight together.
+constexpr int kFinishBatch = 4;
+
+template <int DIAL, bool MIXED>
+__global__ void __launch_bounds__(kTile) k_node_tiles(const DevMesh m, const ClusterPlan p, const NodeTilePlan q,
+                                                    const DevState s, const StepScalars sc) {
+    using R = typename Real<MIXED>::T;
+    using L = TileLayout<MIXED>;
+    constexpr int CS = contrib_stride<MIXED>();
+    constexpr int S = contrib_slot<MIXED>();
+    const int gstep = global_step(s.err, sc.step);
+    if (stale(s.err, gstep)) return;  // uniform over the grid
+    double dial = 0.0, lam = 0.0, pw = 0.0;
+    if (DIAL == DIAL_LCE) {
+        dial = s.dials[3 * gstep];
+        lam = s.dials[3 * gstep + 1];
+        pw = s.dials[3 * gstep + 2];
+    }
+    const double* pos = pos_buf(s, sc.parity);
+    extern __shared__ __align__(128) unsigned char nt_smem[];
+    __shared__ uint64_t bar[2];
+    double* acc = reinterpret_cast<double*>(nt_smem + 2 * q.stride);
+    const int i = threadIdx.x;
+    for (int j = i; j < 3 * q.nodes; j += kTile) acc[j] = 0.0;
+    if (i == 0) {
+        bar_init(&bar[0]);
+        bar_init(&bar[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    // The triangle id of a slot is needed only for per-triangle material,
+    // per-triangle LCE fields or programmed tensors read from arrays.
+    const bool need_t = DIAL != DIAL_LCE || !p.lce_uniform || !m.uniform_hmu;
+    double fmax = -1.0, vmax = -1.0;
+    int fnode = INT_MAX, vnode = INT_MAX;
+    int tile = blockIdx.x;  // the grid is at most the tile count
+    int c = __ldg(q.tile_chunk + tile);
+    if (i == 0) bulk_load(nt_smem, q.rec + (size_t)c * q.stride, __ldg(q.chunk_bytes + c), &bar[0]);
+    int cur = 0;
+    uint32_t phases = 0u;  // bit h: parity of the next phase of half h
+    bool failed = false;
+    for (;;) {
+        const int cend = __ldg(q.tile_chunk + tile + 1);
+        const int ntile = tile + gridDim.x;
+        const int cn = ntile < q.ntiles ? __ldg(q.tile_chunk + ntile) : -1;
+        for (; c < cend; ++c) {
+            // The other half was released by the barrier that ended the
+            // previous chunk.
+            const int nc = c + 1 < cend ? c + 1 : cn;
+            if (i == 0 && nc >= 0)
+                bulk_load(nt_smem + (cur ^ 1) * q.stride, q.rec + (size_t)nc * q.stride, __ldg(q.chunk_bytes + nc),
+                          &bar[cur ^ 1]);
+            const int ok = __syncthreads_and(bar_wait(&bar[cur], (phases >> cur) & 1u) ? 1 : 0);
+            phases ^= 1u << cur;
+            if (!ok) {
+                // Record the error, give the copy into the other half (if
+                // one was started) a bounded chance to land, and stop.
+                if (i == 0) {
+                    atomicCAS(&s.err->flag, 0, 5);  // MS_ERR_TIMEOUT
+                    if (nc >= 0) bar_wait(&bar[cur ^ 1], (phases >> (cur ^ 1)) & 1u);
+                }
+                failed = true;
+                break;
+            }
+            unsigned char* base = nt_smem + cur * q.stride;
+            const int* sid = reinterpret_cast<const int*>(base);
+            R* scoef = reinterpret_cast<R*>(base + L::ids);
+            const double* saux = reinterpret_cast<const double*>(base + L::ids + L::coef);
+            const int4 hd = *reinterpret_cast<const int4*>(base + L::bytes);  // R, E, ntri
+            int ids[6];
+            R cf[24];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) ids[k] = sid[k * kTile + i];
+#pragma unroll
+            for (int k = 0; k < 24; ++k) cf[k] = scoef[k * kTile + i];
+            const double area = saux[i], c2 = saux[kTile + i], s2 = saux[2 * kTile + i], cs = saux[3 * kTile + i];
+            const bool live = i < hd.z;
+            const int t = (need_t && live) ? __ldg(q.chunk_tri + (size_t)c * kTile + i) : 0;
+            __syncthreads();  // the weight area is free for the contributions now
+            R f[18];
+#pragma unroll
+            for (int j = 0; j < 18; ++j) f[j] = R(0);
+            if (live) tile_tri<DIAL, MIXED>(m, p, pos, dial, lam, pw, t, ids, cf, area, c2, s2, cs, f);
+            stage_contrib<MIXED>(scoef + i * CS, f);
+            __syncthreads();
+            // Runs: one node's entries of this chunk each, distinct nodes, so
+            // the runs of a chunk add in parallel without conflicts.
+            const unsigned short* rn = reinterpret_cast<const unsigned short*>(base + L::bytes + 16);
+            const unsigned short* re = rn + hd.x;
+            const unsigned short* en = re + hd.x;
+            for (int r = i; r < hd.x; r += kTile) {
+                const int j = rn[r];
+                int e = r ? re[r - 1] : 0;
+                const int e1 = re[r];
+                double a0 = acc[3 * j], a1 = acc[3 * j + 1], a2 = acc[3 * j + 2];
+                for (; e < e1; ++e) {
+                    const R* v = scoef + S * en[e];
+                    a0 += (double)v[0];
+                    a1 += (double)v[1];
+                    a2 += (double)v[2];
+                }
+                acc[3 * j] = a0;
+                acc[3 * j + 1] = a1;
+                acc[3 * j + 2] = a2;
+            }
+            // Order these generic-proxy writes before the bulk copy that will
+            // refill this half.
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();  // this half is free for the copy after next
+            cur ^= 1;
+        }
+        if (failed) break;
+        // The tile's nodes: every contribution is in.  Each thread clears
+        // the accumulators it reads, ready for the next tile (whose first
+        // runs come after at least one more block barrier).
+        const int n0 = tile * q.nodes;
+        const int nn = min(q.nodes, m.N - n0);
+        for (int j0 = 0; j0 < nn; j0 += kTile * kFinishBatch) {
+            NodeIn in[kFinishBatch];
+#pragma unroll
+            for (int b = 0; b < kFinishBatch; ++b) {
+                const int j = j0 + b * kTile + i;
+                if (j < nn) in[b] = node_load(m, s, sc, n0 + j);
+            }
+#pragma unroll
+            for (int b = 0; b < kFinishBatch; ++b) {
+                const int j = j0 + b * kTile + i;
+                if (j < nn) {
+                    const double Fx = acc[3 * j], Fy = acc[3 * j + 1], Fz = acc[3 * j + 2];
+                    acc[3 * j] = acc[3 * j + 1] = acc[3 * j + 2] = 0.0;
+                    node_core(m, s, sc, gstep, n0 + j, in[b], Fx, Fy, Fz, fmax, fnode, vmax, vnode);
+                }
+            }
+        }
+        tile = ntile;
+        if (tile >= q.ntiles) break;
+        c = cn;
+    }
+    if (sc.check) {
+        const EqPartial r = eq_block_reduce<kTile>(fmax, fnode, vmax, vnode);
+        eq_store_and_fold(s, r, blockIdx.x, gridDim.x, gridDim.x);
+    }
+}
+
+template <int DIAL, bool MIXED>
+cudaError_t launch_one(const DevMesh& m, const ClusterPlan& p, const NodeTilePlan& q, const DevState& s,
+                       const StepScalars& sc, cudaStream_t st) {
+    const int grid = std::min(q.ntiles, q.grid);
+    if (grid <= 0) return cudaSuccess;
+    k_node_tiles<DIAL, MIXED><<<grid, kTile, node_tile_smem(q.stride, q.nodes), st>>>(m, p, q, s, sc);
+    return cudaGetLastError();
+}
+
+template <int DIAL, bool MIXED>
+cudaError_t prepare_one(size_t smem, int& blocks) {
+    cudaError_t e =
+        cudaFuncSetAttribute(k_node_tiles<DIAL, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int b = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_node_tiles<DIAL, MIXED>, kTile, smem);
+    if (e != cudaSuccess) return e;
+    blocks = blocks == 0 ? b : std::min(blocks, b);
+    return cudaSuccess;
+}
+
+}  // namespace
+
+size_t node_tile_smem(size_t stride, int nodes) { return 2 * stride + 24 * (size_t)nodes; }
+
+cudaError_t prepare_node_tile_kernels(int mixed, size_t smem, int* blocks_per_sm) {
+    int b = 0;
+    cudaError_t e = mixed ? prepare_one<DIAL_LCE, true>(smem, b) : prepare_one<DIAL_LCE, false>(smem, b);
+    if (e == cudaSuccess) e = mixed ? prepare_one<DIAL_ARRAYS, true>(smem, b) : prepare_one<DIAL_ARRAYS, false>(smem, b);
+    *blocks_per_sm = b;
+    return e;
+}
+
+cudaError_t launch_node_tiles(const DevMesh& m, const ClusterPlan& p, const NodeTilePlan& q, const DevState& s,
+                              const StepScalars& sc, int dial_mode, int mixed, cudaStream_t st) {
+    if (dial_mode == DIAL_LCE)
+        return mixed ? launch_one<DIAL_LCE, true>(m, p, q, s, sc, st) : launch_one<DIAL_LCE, false>(m, p, q, s, sc, st);
+    return mixed ? launch_one<DIAL_ARRAYS, true>(m, p, q, s, sc, st) : launch_one<DIAL_ARRAYS, false>(m, p, q, s, sc, st);
+}
+
+}  // namespace msb

@@ -105,26 +105,47 @@ __device__ __forceinline__ void eq_store_and_fold(const DevState& s, const EqPar
     }
 }
 
+// A node's state as the step reads it: position and velocity from the
+// step's buffer, dof mass, constraint flag.
+struct NodeIn {
+    double px, py, pz, vx, vy, vz, mass;
+    int fixed;
+};
+
+__device__ __forceinline__ NodeIn node_load(const DevMesh& m, const DevState& s, const StepScalars& sc, int n) {
+    const int N = m.N;
+    const double* pos = pos_buf(s, sc.parity);
+    const double* vel = vel_buf(s, sc.parity);
+    NodeIn in;
+    in.px = pos[n];
+    in.py = pos[N + n];
+    in.pz = pos[2 * N + n];
+    in.vx = vel[n];
+    in.vy = vel[N + n];
+    in.vz = vel[2 * N + n];
+    in.mass = __ldg(m.mass + n);
+    in.fixed = __ldg(m.fixed + n);
+    return in;
+}
+
 // Everything after the deformation-force sum for one node: damping
 // (calc_non_deformation_forces.cpp:44-57), constraints (impose_constraints.cpp:56-68),
 // the equilibrium maxima (is_at_equilibrium.cpp:62-76), the force guard and
 // the symplectic-Euler update (advance_dynamics.cpp:58-93) into the other
-// ping-pong buffer.
-__device__ __forceinline__ void node_finish(const DevMesh& m, const DevState& s, const StepScalars& sc, int gstep,
-                                            int n, double Fx, double Fy, double Fz, double& fmax, int& fnode,
-                                            double& vmax, int& vnode) {
+// ping-pong buffer, from the node's loaded state.
+__device__ __forceinline__ void node_core(const DevMesh& m, const DevState& s, const StepScalars& sc, int gstep,
+                                          int n, const NodeIn& in, double Fx, double Fy, double Fz, double& fmax,
+                                          int& fnode, double& vmax, int& vnode) {
     const int N = m.N;
-    const double* pos = pos_buf(s, sc.parity);
-    const double* vel = vel_buf(s, sc.parity);
-    const double vx = vel[n], vy = vel[N + n], vz = vel[2 * N + n];
-    const double mass = __ldg(m.mass + n);
+    const double vx = in.vx, vy = in.vy, vz = in.vz;
+    const double mass = in.mass;
     if (!sc.gd) {
         const double dm = -sc.damping * mass;
         Fx += dm * vx / sc.rho_hh;
         Fy += dm * vy / sc.rho_hh;
         Fz += dm * vz / sc.rho_hh;
     }
-    if (__ldg(m.fixed + n)) Fx = Fy = Fz = 0.0;
+    if (in.fixed) Fx = Fy = Fz = 0.0;
     if (sc.check) {
         eq_merge(fmax, fnode, sqrt(Fx * Fx + Fy * Fy + Fz * Fz), n);
         eq_merge(vmax, vnode, sqrt(vx * vx + vy * vy + vz * vz), n);
@@ -147,12 +168,18 @@ __device__ __forceinline__ void node_finish(const DevMesh& m, const DevState& s,
     }
     double* npos = pos_buf(s, sc.parity ^ 1);
     double* nvel = vel_buf(s, sc.parity ^ 1);
-    npos[n] = pos[n] + sc.dt * nvx;
-    npos[N + n] = pos[N + n] + sc.dt * nvy;
-    npos[2 * N + n] = pos[2 * N + n] + sc.dt * nvz;
+    npos[n] = in.px + sc.dt * nvx;
+    npos[N + n] = in.py + sc.dt * nvy;
+    npos[2 * N + n] = in.pz + sc.dt * nvz;
     nvel[n] = nvx;
     nvel[N + n] = nvy;
     nvel[2 * N + n] = nvz;
+}
+
+__device__ __forceinline__ void node_finish(const DevMesh& m, const DevState& s, const StepScalars& sc, int gstep,
+                                            int n, double Fx, double Fy, double Fz, double& fmax, int& fnode,
+                                            double& vmax, int& vnode) {
+    node_core(m, s, sc, gstep, n, node_load(m, s, sc, n), Fx, Fy, Fz, fmax, fnode, vmax, vnode);
 }
 
 // Entries whose indices, then contributions, one thread loads together.

@@ -58,6 +58,46 @@ __device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t parity) {
 }
 
 
+// One triangle of a tile record: its material and programmed metric (protocol
+// 3 in-kernel from the step's dial, lambda, lambda^(-2 nu) triple, or the
+// abar/bbar arrays), the gather of its 6 patch nodes and its 18
+// contributions.  Shared by every kernel that walks tile records, so they
+// give the same bits.
+template <int DIAL, bool MIXED>
+__device__ __forceinline__ void tile_tri(const DevMesh& m, const ClusterPlan& p, const double* __restrict__ pos,
+                                         double dial, double lam, double pw, int t, const int (&ids)[6],
+                                         const typename tridev::Real<MIXED>::T (&c)[24], double area, double c2,
+                                         double s2, double cs, typename tridev::Real<MIXED>::T (&f)[18]) {
+    dev::TriMat<double> mt;
+    tridev::tri_hmu(m, t, mt.h, mt.mu);
+    mt.area = area;
+    if (DIAL == DIAL_LCE) {
+        double l2 = __dmul_rn(lam, lam), pp = pw;
+        if (!p.lce_uniform) {
+            const double2 ln = __ldg(p.lce_ln + t);
+            const double lt = (1.0 - dial) * 1.0 + dial * ln.x;
+            l2 = __dmul_rn(lt, lt);
+            pp = pow(lt, -2.0 * ln.y);
+        }
+        tridev::lce_metric(c2, s2, cs, l2, pp, mt);
+    } else {
+        mt.abar0 = __ldg(m.abar + t);
+        mt.abar1 = __ldg(m.abar + (size_t)m.T + t);
+        mt.abar2 = __ldg(m.abar + 2 * (size_t)m.T + t);
+        mt.bbar0 = __ldg(m.bbar + t);
+        mt.bbar1 = __ldg(m.bbar + (size_t)m.T + t);
+        mt.bbar2 = __ldg(m.bbar + 2 * (size_t)m.T + t);
+    }
+    double P[6][3];
+#pragma unroll
+    for (int sl = 0; sl < 6; ++sl) {
+        P[sl][0] = __ldg(pos + ids[sl]);
+        P[sl][1] = __ldg(pos + m.N + ids[sl]);
+        P[sl][2] = __ldg(pos + 2 * m.N + ids[sl]);
+    }
+    tridev::tri_forces<MIXED>(P, c, mt, m.nu, m.gamma, f);
+}
+
 // Walks this block's tiles (blockIdx.x, then every gridDim.x-th) of T
 // triangles.  Thread 0 brings the next tile's record into the other half of
 // a double buffer with one bulk copy while the block works on the current

@@ -45,36 +45,7 @@ __global__ void __launch_bounds__(kTile) k_tri_tiles(const DevMesh m, const Clus
     else out = s.contrib;
     tile_loop<MIXED>(m.T, tl, out, &s.err->flag,
                      [&](int t, const int (&ids)[6], const R (&c)[24], double area, double c2, double s2, double cs,
-                         R (&f)[18]) {
-                         TriMat<double> mt;
-                         tri_hmu(m, t, mt.h, mt.mu);
-                         mt.area = area;
-                         if (DIAL == DIAL_LCE) {
-                             double l2 = __dmul_rn(lam, lam), pp = pw;
-                             if (!p.lce_uniform) {
-                                 const double2 ln = __ldg(p.lce_ln + t);
-                                 const double lt = (1.0 - dial) * 1.0 + dial * ln.x;
-                                 l2 = __dmul_rn(lt, lt);
-                                 pp = pow(lt, -2.0 * ln.y);
-                             }
-                             lce_metric(c2, s2, cs, l2, pp, mt);
-                         } else {
-                             mt.abar0 = __ldg(m.abar + t);
-                             mt.abar1 = __ldg(m.abar + (size_t)m.T + t);
-                             mt.abar2 = __ldg(m.abar + 2 * (size_t)m.T + t);
-                             mt.bbar0 = __ldg(m.bbar + t);
-                             mt.bbar1 = __ldg(m.bbar + (size_t)m.T + t);
-                             mt.bbar2 = __ldg(m.bbar + 2 * (size_t)m.T + t);
-                         }
-                         double P[6][3];
-#pragma unroll
-                         for (int sl = 0; sl < 6; ++sl) {
-                             P[sl][0] = __ldg(pos + ids[sl]);
-                             P[sl][1] = __ldg(pos + m.N + ids[sl]);
-                             P[sl][2] = __ldg(pos + 2 * m.N + ids[sl]);
-                         }
-                         tri_forces<MIXED>(P, c, mt, m.nu, m.gamma, f);
-                     });
+                         R (&f)[18]) { tile_tri<DIAL, MIXED>(m, p, pos, dial, lam, pw, t, ids, c, area, c2, s2, cs, f); });
 }
 
 template <int DIAL, bool MIXED>
