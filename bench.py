@@ -260,8 +260,11 @@ def run_ours(args):
     T = model.num_tris
     prec = MS_PRECISION_MIXED if args.precision == "mixed" else MS_PRECISION_FP64
     g = GpuLoop(model, precision=prec, device=local)
-    g.set_step_path({"cluster": 0, "two-kernel": 1, "tiles": 2, "node-tiles": 3}[args.path])
+    names = {"cluster": 0, "two-kernel": 1, "tiles": 2, "node-tiles": 3}
+    if args.path != "auto":
+        g.set_step_path(names[args.path])
     plan = g.plan_info()
+    args.path = {v: k for k, v in names.items()}[plan["path"]]
     g.set_programmed(3, info, bbar, s.dial_factors_to_hold_at_spacing)
     g.upload(model.dofs(1))
     dials = dial_sequence(model, args.warmup + args.steps + 64)
@@ -508,8 +511,8 @@ def main():
     ap.add_argument("--workload", default="disk1p8m")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
-    ap.add_argument("--path", choices=["cluster", "two-kernel", "tiles", "node-tiles"], default="tiles",
-                    help="fused-step implementation (ms_set_step_path)")
+    ap.add_argument("--path", choices=["auto", "cluster", "two-kernel", "tiles", "node-tiles"], default="auto",
+                    help="fused-step implementation (ms_set_step_path); auto: the library's default")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -204,13 +204,14 @@ void* ms_stream(ms_handle* h);
  * thread-block cluster owns a Morton tile of triangles, keeps their force
  * contributions in distributed shared memory and updates the tile's
  * interior nodes itself; 1 the two-kernel step (per-triangle kernel writes
- * all contributions to HBM, per-node kernel gathers them); 2 (default) the
- * two-kernel step whose per-triangle kernel is persistent and streams its
- * tables through shared memory with bulk asynchronous copies; 3 the
- * node-tiled step -- one kernel: each block takes tiles of consecutive
- * nodes, computes every triangle that touches the tile (border triangles
- * once per tile), sums the tile's forces in shared memory and updates its
- * nodes, so no contribution goes through HBM.  All sum every node's
+ * all contributions to HBM, per-node kernel gathers them); 2 the two-kernel
+ * step whose per-triangle kernel is persistent and streams its tables
+ * through shared memory with bulk asynchronous copies; 3 the node-tiled
+ * step -- one kernel: each block takes tiles of consecutive nodes, computes
+ * every triangle that touches the tile (border triangles once per tile),
+ * sums the tile's forces in shared memory and updates its nodes, so no
+ * contribution goes through HBM.  The default is 3 on meshes with at least
+ * one node tile per resident block, else 2.  All sum every node's
  * contributions in ascending triangle order, so they give the same bits. */
 ms_status ms_set_step_path(ms_handle* h, int path);
 /* Tiling of the cluster path: CTAs per cluster, triangles per CTA, number of
@@ -219,6 +220,10 @@ ms_status ms_set_step_path(ms_handle* h, int path);
 ms_status ms_plan_info(ms_handle* h, int* cluster_size, int* tris_per_cta, int* clusters, int* halo_nodes,
                        int* path);
 
+/* The node-tiled step's plan on this handle: nodes per tile, tiles, chunk
+ * records and persistent blocks per launch (all 0 when the path is
+ * unavailable). */
+ms_status ms_node_tile_plan(ms_handle* h, int* nodes_per_tile, int* tiles, int* chunks, int* blocks);
 /* Layout of the node-tiled step (path 3) for a mesh and a tile size, computed
  * on the host alone (no device needed), with the same code and the same
  * bounds checks ms_create runs: node tiles, chunk records (128 triangle

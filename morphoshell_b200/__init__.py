@@ -27,7 +27,7 @@ GPU_SYMBOLS = [
     "ms_download_programmed", "ms_surface_derivs", "ms_a_b_normals", "ms_deformation_forces",
     "ms_non_deformation_forces", "ms_impose_constraints", "ms_is_at_equilibrium", "ms_advance_dynamics",
     "ms_step_n", "ms_output_quantities", "ms_device_info", "ms_stream", "ms_time_kernels",
-    "ms_deformation_forces_noalloc", "ms_set_step_path", "ms_plan_info", "ms_node_tile_layout",
+    "ms_deformation_forces_noalloc", "ms_set_step_path", "ms_plan_info", "ms_node_tile_layout", "ms_node_tile_plan",
     "ms_batch_create", "ms_batch_destroy", "ms_batch_last_error", "ms_batch_run", "ms_batch_status",
     "ms_batch_download_dofs", "ms_batch_upload_dofs", "ms_batch_set_schedule", "ms_batch_get_schedule",
     "ms_batch_autotune", "ms_batch_info", "ms_batch_stream", "ms_batch_set_start",
@@ -168,6 +168,7 @@ def lib() -> C.CDLL:
         L.ms_set_step_path.argtypes = [C.c_void_p, C.c_int]
         ip = C.POINTER(C.c_int)
         L.ms_plan_info.argtypes = [C.c_void_p, ip, ip, ip, ip, ip]
+        L.ms_node_tile_plan.argtypes = [C.c_void_p, ip, ip, ip, ip]
         L.ms_node_tile_layout.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, P(ms_node_tile_info)]
         L.ms_stream.argtypes = [C.c_void_p]
         L.ms_stream.restype = C.c_void_p
@@ -440,13 +441,18 @@ class GpuLoop:
     def set_step_path(self, path: int):
         """0: cluster-tiled step, 1: two-kernel step, 2: two-kernel step with
         the per-triangle tables fed by bulk asynchronous copies, 3: node-tiled
-        one-kernel step (forces summed in shared memory per tile of nodes)."""
+        one-kernel step (forces summed in shared memory per tile of nodes;
+        the default on meshes with a node tile for every resident block)."""
         self._chk(lib().ms_set_step_path(self._h, path), "set_step_path")
 
     def plan_info(self) -> dict:
         v = [C.c_int() for _ in range(5)]
         self._chk(lib().ms_plan_info(self._h, *[C.byref(x) for x in v]), "plan_info")
-        return dict(zip(["cluster_size", "tris_per_cta", "clusters", "halo_nodes", "path"], [x.value for x in v]))
+        out = dict(zip(["cluster_size", "tris_per_cta", "clusters", "halo_nodes", "path"], [x.value for x in v]))
+        w = [C.c_int() for _ in range(4)]
+        self._chk(lib().ms_node_tile_plan(self._h, *[C.byref(x) for x in w]), "node_tile_plan")
+        out.update(zip(["nodes_per_tile", "node_tiles", "node_tile_chunks", "node_tile_blocks"], [x.value for x in w]))
+        return out
 
     def stream(self) -> int:
         """cudaStream_t of this handle, as an integer."""

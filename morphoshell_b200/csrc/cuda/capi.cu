@@ -71,7 +71,7 @@ struct ms_handle {
     ClusterPlan plan{};
     bool have_plan = false;
     bool have_cluster = false;
-    int step_path = 1;  // 0 cluster-tiled, 1 two-kernel, 2 two-kernel with bulk-copied tiles (default when built)
+    int step_path = 1;  // 0 cluster-tiled, 1 two-kernel, 2 two-kernel with bulk-copied tiles, 3 node-tiled
     std::vector<double> area_host;
     double lce_lam_final = 0, lce_nu = 0;
     int halo_parts = 0;
@@ -227,10 +227,6 @@ ms_status build_tiles(ms_handle* h, const ms_mesh_desc* d) {
     return MS_OK;
 }
 
-#ifndef MSB_NT_NODES
-#define MSB_NT_NODES 1024
-#endif
-
 // Host-side layout of the node-tiled step (NodeTilePlan) for tiles of NT
 // consecutive nodes: every tile's triangle list (ascending t), its chunks and
 // their node sections, checked against the bounds the kernel relies on.
@@ -346,31 +342,60 @@ bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, con
     return true;
 }
 
+// Largest nodes per tile of the node-tiled step: the largest tiles (fewest
+// border triangles computed twice) whose blocks still fit 3 (FP64) or 4
+// (mixed) to an SM; and the smallest tiles worth their border.
 #ifndef MSB_NT_NODES
-#define MSB_NT_NODES 1024
+#define MSB_NT_NODES 928
 #endif
+#ifndef MSB_NT_NODES_MIXED
+#define MSB_NT_NODES_MIXED 1008
+#endif
+constexpr int kNtNodesMin = 256;
 
-// Plan of the node-tiled step for tiles of MSB_NT_NODES nodes: the chunk
-// records, area in the trigonometry block (cos^2 = 1, the rest 0) until
-// prepare_lce_tables writes the director's values.  Leaves the other paths in
-// place when the kernel cannot be set up.
+// Plan of the node-tiled step: the chunk records, area in the trigonometry
+// block (cos^2 = 1, the rest 0) until prepare_lce_tables writes the
+// director's values.  A block walks its tiles in turn, so the step takes as
+// long as the block with the most tiles: the tile size is chosen so that the
+// tile count is a multiple of the resident blocks (SMs x blocks per SM), at
+// the largest size that keeps those blocks resident.  Leaves the other paths
+// in place when the kernel cannot be set up.
 ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vector<int>& off,
                            const std::vector<int>& ent) {
-    const int N = d->num_nodes, T = d->num_tris, NT = MSB_NT_NODES;
     const int mixed = h->precision == MS_PRECISION_MIXED;
+    const int N = d->num_nodes, T = d->num_tris;
     if (N <= 0 || T <= 0) return MS_OK;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int target = node_tile_blocks_target(mixed);
+    int nt_max = mixed ? MSB_NT_NODES_MIXED : MSB_NT_NODES;
     NodeTileLayout L;
     std::string err;
-    if (!node_tile_layout(d->patch_ids, N, T, NT, mixed, off, ent, L, err)) return fail(h, MS_ERR_INVALID_ARGUMENT, err);
-    const int K = L.K, C = L.C;
-    const size_t stride = L.stride, fixed = L.fixed;
-    const size_t smem = node_tile_smem(stride, NT);
-    int blocks = 0;
-    if (smem > 227 * 1024 || prepare_node_tile_kernels(mixed, smem, &blocks) != cudaSuccess || blocks <= 0) {
-        cudaGetLastError();
+    int NT = 0, blocks = 0;
+    size_t smem = 0;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        const long long slots = (long long)std::max(sms, 1) * target;
+        const long long k = std::max(1LL, (N + slots * nt_max - 1) / (slots * nt_max));
+        NT = std::max(std::min(nt_max, kNtNodesMin), (int)((N + k * slots - 1) / (k * slots)));
+        L = NodeTileLayout();
+        if (!node_tile_layout(d->patch_ids, N, T, NT, mixed, off, ent, L, err))
+            return fail(h, MS_ERR_INVALID_ARGUMENT, err);
+        smem = node_tile_smem(L.stride, NT, mixed);
+        blocks = 0;
+        if (smem > 227 * 1024 || prepare_node_tile_kernels(mixed, smem, &blocks) != cudaSuccess) {
+            cudaGetLastError();
+            blocks = 0;
+        }
+        if (blocks >= target) break;
+        nt_max = nt_max * 7 / 8;
+    }
+    if (blocks <= 0) {
         h->have_ntiles = false;
         return MS_OK;  // the other paths remain
     }
+    const int K = L.K, C = L.C;
+    const size_t stride = L.stride, fixed = L.fixed;
     std::vector<unsigned char> buf(stride * C, 0);
     std::vector<int>& ctri = h->nt_chunk_tri;
     ctri.assign((size_t)C * kTile, -1);
@@ -415,9 +440,6 @@ ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vecto
     MS_TRY(upload(h, &d_tile_chunk, L.tile_chunk));
     MS_TRY(upload(h, &d_bytes, L.bytes));
     MS_TRY(upload(h, &d_ctri, ctri));
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     NodeTilePlan& q = h->ntp;
     q.nodes = NT;
     q.ntiles = K;
@@ -438,6 +460,9 @@ ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vecto
         h->s.eq_blocks = parts;
     }
     h->have_ntiles = true;
+    // Measured fastest on B200 once every block has a tile of its own
+    // (same bits as paths 1 and 2).
+    if (K >= q.grid) h->step_path = 3;
     return MS_OK;
 }
 
@@ -1225,6 +1250,16 @@ ms_status ms_plan_info(ms_handle* h, int* cluster_size, int* tris_per_cta, int* 
     return MS_OK;
 }
 
+ms_status ms_node_tile_plan(ms_handle* h, int* nodes_per_tile, int* tiles, int* chunks, int* blocks) {
+    if (!h) return MS_ERR_INVALID_ARGUMENT;
+    const bool ok = h->have_ntiles;
+    if (nodes_per_tile) *nodes_per_tile = ok ? h->ntp.nodes : 0;
+    if (tiles) *tiles = ok ? h->ntp.ntiles : 0;
+    if (chunks) *chunks = ok ? h->ntp.nchunks : 0;
+    if (blocks) *blocks = ok ? std::min(h->ntp.ntiles, h->ntp.grid) : 0;
+    return MS_OK;
+}
+
 ms_status ms_node_tile_layout(int num_nodes, int num_tris, const int* patch_ids, int nodes_per_tile, int precision,
                               ms_node_tile_info* out) {
     if (num_nodes <= 0 || num_tris <= 0 || !patch_ids || !out) return MS_ERR_INVALID_ARGUMENT;
@@ -1249,7 +1284,7 @@ ms_status ms_node_tile_layout(int num_nodes, int num_tris, const int* patch_ids,
     long long b = 0;
     for (unsigned x : L.bytes) b += x;
     out->bytes_per_step = b;
-    out->shared_bytes = (long long)node_tile_smem(L.stride, nodes_per_tile);
+    out->shared_bytes = (long long)node_tile_smem(L.stride, nodes_per_tile, precision == MS_PRECISION_MIXED);
     return MS_OK;
 }
 

@@ -280,7 +280,8 @@ cudaError_t launch_tri_tiles(const DevMesh& m, const ClusterPlan& p, const DevSt
                              int dial_mode, int mixed, cudaStream_t st);
 // Node-tiled step (node_tiles.cu): shared memory per block for a plan,
 // kernel set-up (dynamic shared memory; resident blocks per SM) and launch.
-size_t node_tile_smem(size_t stride, int nodes);
+size_t node_tile_smem(size_t stride, int nodes, int mixed);
+int node_tile_blocks_target(int mixed);
 cudaError_t prepare_node_tile_kernels(int mixed, size_t smem, int* blocks_per_sm);
 cudaError_t launch_node_tiles(const DevMesh& m, const ClusterPlan& p, const NodeTilePlan& q, const DevState& s,
                               const StepScalars& sc, int dial_mode, int mixed, cudaStream_t st);

@@ -37,14 +37,40 @@ using namespace stepdev;
 using namespace tridev;
 using namespace tiles;
 
-// Nodes finished per thread with their loads in flight together.
-constexpr int kFinishBatch = 4;
+// Nodes finished per thread with their loads in flight together (more than
+// one spills at the register budget of 3 or 4 blocks per SM).
+constexpr int kFinishBatch = 1;
+
+// Shared memory of a block: the chunk's fixed part (ids, weights,
+// trigonometry; single-buffered: it is refilled as soon as every thread holds
+// its triangle's tables in registers), the contribution staging area, two
+// node sections (the current chunk's, and the next one landing) and the
+// tile's per-node accumulators.
+template <bool MIXED>
+struct NtSmem {
+    static constexpr size_t fixed = TileLayout<MIXED>::bytes;
+    static constexpr size_t stage = (size_t)kTile * contrib_stride<MIXED>() * (MIXED ? 4 : 8);
+    __host__ __device__ static size_t ns_cap(size_t stride) { return stride - fixed; }
+    __host__ __device__ static size_t bytes(size_t stride, int nodes) {
+        return fixed + stage + 2 * ns_cap(stride) + 24 * (size_t)nodes;
+    }
+};
+
+// Resident blocks asked of the compiler (registers): FP64 at 3 per SM (168
+// registers), mixed at 4 (128).
+#ifndef MSB_NT_MINB
+#define MSB_NT_MINB 3
+#endif
+#ifndef MSB_NT_MINB_MIXED
+#define MSB_NT_MINB_MIXED 4
+#endif
 
 template <int DIAL, bool MIXED>
-__global__ void __launch_bounds__(kTile) k_node_tiles(const DevMesh m, const ClusterPlan p, const NodeTilePlan q,
-                                                    const DevState s, const StepScalars sc) {
+__global__ void __launch_bounds__(kTile, MIXED ? MSB_NT_MINB_MIXED : MSB_NT_MINB)
+    k_node_tiles(const DevMesh m, const ClusterPlan p, const NodeTilePlan q, const DevState s, const StepScalars sc) {
     using R = typename Real<MIXED>::T;
     using L = TileLayout<MIXED>;
+    using SM = NtSmem<MIXED>;
     constexpr int CS = contrib_stride<MIXED>();
     constexpr int S = contrib_slot<MIXED>();
     const int gstep = global_step(s.err, sc.step);
@@ -57,16 +83,36 @@ __global__ void __launch_bounds__(kTile) k_node_tiles(const DevMesh m, const Clu
     }
     const double* pos = pos_buf(s, sc.parity);
     extern __shared__ __align__(128) unsigned char nt_smem[];
-    __shared__ uint64_t bar[2];
-    double* acc = reinterpret_cast<double*>(nt_smem + 2 * q.stride);
+    __shared__ uint64_t bar;
+    const size_t ns_cap = SM::ns_cap(q.stride);
+    unsigned char* fx = nt_smem;
+    R* stage = reinterpret_cast<R*>(nt_smem + SM::fixed);
+    unsigned char* nsec = nt_smem + SM::fixed + SM::stage;
+    double* acc = reinterpret_cast<double*>(nsec + 2 * ns_cap);
     const int i = threadIdx.x;
     for (int j = i; j < 3 * q.nodes; j += kTile) acc[j] = 0.0;
     if (i == 0) {
-        bar_init(&bar[0]);
-        bar_init(&bar[1]);
+        bar_init(&bar);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    // Thread 0: chunk c's fixed part into the fixed area and its node section
+    // into node-section slot `slot`, both counted on the one barrier.
+    auto fetch = [&](int c, int slot) {
+        const unsigned char* src = q.rec + (size_t)c * q.stride;
+        const uint32_t nb = __ldg(q.chunk_bytes + c) - (uint32_t)SM::fixed;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)),
+                     "r"((uint32_t)SM::fixed + nb)
+                     : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_addr(fx)),
+                     "l"(src), "r"((uint32_t)SM::fixed), "r"(smem_addr(&bar))
+                     : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_addr(nsec + slot * ns_cap)),
+                     "l"(src + SM::fixed), "r"(nb), "r"(smem_addr(&bar))
+                     : "memory");
+    };
     // The triangle id of a slot is needed only for per-triangle material,
     // per-triangle LCE fields or programmed tensors read from arrays.
     const bool need_t = DIAL != DIAL_LCE || !p.lce_uniform || !m.uniform_hmu;
@@ -74,38 +120,31 @@ __global__ void __launch_bounds__(kTile) k_node_tiles(const DevMesh m, const Clu
     int fnode = INT_MAX, vnode = INT_MAX;
     int tile = blockIdx.x;  // the grid is at most the tile count
     int c = __ldg(q.tile_chunk + tile);
-    if (i == 0) bulk_load(nt_smem, q.rec + (size_t)c * q.stride, __ldg(q.chunk_bytes + c), &bar[0]);
-    int cur = 0;
-    uint32_t phases = 0u;  // bit h: parity of the next phase of half h
+    if (i == 0) fetch(c, 0);
+    uint32_t phase = 0u;
+    int slot = 0;  // node-section slot of the current chunk
     bool failed = false;
     for (;;) {
         const int cend = __ldg(q.tile_chunk + tile + 1);
         const int ntile = tile + gridDim.x;
         const int cn = ntile < q.ntiles ? __ldg(q.tile_chunk + ntile) : -1;
         for (; c < cend; ++c) {
-            // The other half was released by the barrier that ended the
-            // previous chunk.
             const int nc = c + 1 < cend ? c + 1 : cn;
-            if (i == 0 && nc >= 0)
-                bulk_load(nt_smem + (cur ^ 1) * q.stride, q.rec + (size_t)nc * q.stride, __ldg(q.chunk_bytes + nc),
-                          &bar[cur ^ 1]);
-            const int ok = __syncthreads_and(bar_wait(&bar[cur], (phases >> cur) & 1u) ? 1 : 0);
-            phases ^= 1u << cur;
+            // This barrier also ends the previous chunk's runs, so the
+            // staging area and the other node-section slot are free after it.
+            const int ok = __syncthreads_and(bar_wait(&bar, phase) ? 1 : 0);
+            phase ^= 1u;
             if (!ok) {
-                // Record the error, give the copy into the other half (if
-                // one was started) a bounded chance to land, and stop.
-                if (i == 0) {
-                    atomicCAS(&s.err->flag, 0, 5);  // MS_ERR_TIMEOUT
-                    if (nc >= 0) bar_wait(&bar[cur ^ 1], (phases >> (cur ^ 1)) & 1u);
-                }
+                // No other copy is in flight (the next one starts below).
+                if (i == 0) atomicCAS(&s.err->flag, 0, 5);  // MS_ERR_TIMEOUT
                 failed = true;
                 break;
             }
-            unsigned char* base = nt_smem + cur * q.stride;
-            const int* sid = reinterpret_cast<const int*>(base);
-            R* scoef = reinterpret_cast<R*>(base + L::ids);
-            const double* saux = reinterpret_cast<const double*>(base + L::ids + L::coef);
-            const int4 hd = *reinterpret_cast<const int4*>(base + L::bytes);  // R, E, ntri
+            const unsigned char* ns = nsec + slot * ns_cap;
+            const int4 hd = *reinterpret_cast<const int4*>(ns);  // R, E, ntri
+            const int* sid = reinterpret_cast<const int*>(fx);
+            const R* scoef = reinterpret_cast<const R*>(fx + L::ids);
+            const double* saux = reinterpret_cast<const double*>(fx + L::ids + L::coef);
             int ids[6];
             R cf[24];
 #pragma unroll
@@ -115,16 +154,19 @@ __global__ void __launch_bounds__(kTile) k_node_tiles(const DevMesh m, const Clu
             const double area = saux[i], c2 = saux[kTile + i], s2 = saux[2 * kTile + i], cs = saux[3 * kTile + i];
             const bool live = i < hd.z;
             const int t = (need_t && live) ? __ldg(q.chunk_tri + (size_t)c * kTile + i) : 0;
-            __syncthreads();  // the weight area is free for the contributions now
+            // Order these reads before the bulk copy that refills the area.
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            if (i == 0 && nc >= 0) fetch(nc, slot ^ 1);
             R f[18];
 #pragma unroll
             for (int j = 0; j < 18; ++j) f[j] = R(0);
             if (live) tile_tri<DIAL, MIXED>(m, p, pos, dial, lam, pw, t, ids, cf, area, c2, s2, cs, f);
-            stage_contrib<MIXED>(scoef + i * CS, f);
+            stage_contrib<MIXED>(stage + i * CS, f);
             __syncthreads();
             // Runs: one node's entries of this chunk each, distinct nodes, so
             // the runs of a chunk add in parallel without conflicts.
-            const unsigned short* rn = reinterpret_cast<const unsigned short*>(base + L::bytes + 16);
+            const unsigned short* rn = reinterpret_cast<const unsigned short*>(ns + 16);
             const unsigned short* re = rn + hd.x;
             const unsigned short* en = re + hd.x;
             for (int r = i; r < hd.x; r += kTile) {
@@ -133,7 +175,7 @@ __global__ void __launch_bounds__(kTile) k_node_tiles(const DevMesh m, const Clu
                 const int e1 = re[r];
                 double a0 = acc[3 * j], a1 = acc[3 * j + 1], a2 = acc[3 * j + 2];
                 for (; e < e1; ++e) {
-                    const R* v = scoef + S * en[e];
+                    const R* v = stage + S * en[e];
                     a0 += (double)v[0];
                     a1 += (double)v[1];
                     a2 += (double)v[2];
@@ -142,16 +184,17 @@ __global__ void __launch_bounds__(kTile) k_node_tiles(const DevMesh m, const Clu
                 acc[3 * j + 1] = a1;
                 acc[3 * j + 2] = a2;
             }
-            // Order these generic-proxy writes before the bulk copy that will
-            // refill this half.
+            // Generic reads of this node-section slot come before the copy
+            // that refills it two chunks on.
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();  // this half is free for the copy after next
-            cur ^= 1;
+            slot ^= 1;
         }
         if (failed) break;
-        // The tile's nodes: every contribution is in.  Each thread clears
-        // the accumulators it reads, ready for the next tile (whose first
-        // runs come after at least one more block barrier).
+        // The tile's nodes: every contribution is in once the runs of the
+        // last chunk are done.  Each thread clears the accumulators it reads,
+        // ready for the next tile (whose first runs come after at least two
+        // more block barriers).
+        __syncthreads();
         const int n0 = tile * q.nodes;
         const int nn = min(q.nodes, m.N - n0);
         for (int j0 = 0; j0 < nn; j0 += kTile * kFinishBatch) {
@@ -186,7 +229,7 @@ cudaError_t launch_one(const DevMesh& m, const ClusterPlan& p, const NodeTilePla
                        const StepScalars& sc, cudaStream_t st) {
     const int grid = std::min(q.ntiles, q.grid);
     if (grid <= 0) return cudaSuccess;
-    k_node_tiles<DIAL, MIXED><<<grid, kTile, node_tile_smem(q.stride, q.nodes), st>>>(m, p, q, s, sc);
+    k_node_tiles<DIAL, MIXED><<<grid, kTile, NtSmem<MIXED>::bytes(q.stride, q.nodes), st>>>(m, p, q, s, sc);
     return cudaGetLastError();
 }
 
@@ -204,7 +247,11 @@ cudaError_t prepare_one(size_t smem, int& blocks) {
 
 }  // namespace
 
-size_t node_tile_smem(size_t stride, int nodes) { return 2 * stride + 24 * (size_t)nodes; }
+size_t node_tile_smem(size_t stride, int nodes, int mixed) {
+    return mixed ? NtSmem<true>::bytes(stride, nodes) : NtSmem<false>::bytes(stride, nodes);
+}
+
+int node_tile_blocks_target(int mixed) { return mixed ? MSB_NT_MINB_MIXED : MSB_NT_MINB; }
 
 cudaError_t prepare_node_tile_kernels(int mixed, size_t smem, int* blocks_per_sm) {
     int b = 0;

@@ -126,3 +126,16 @@ def test_node_tiles_kernel_timing(workdir):
     g.upload(x, v)
     t_tri, t_node = g.time_kernels(5, 0.2, s.timestep, s.damping_factor_1)
     assert t_tri > 0 and t_node == 0
+
+
+def test_node_tile_plan_balances_blocks(workdir):
+    """The tile count is a multiple of the persistent blocks (or the tiles
+    are at their smallest size), so no block walks more tiles than another
+    by more than one."""
+    from morphoshell_b200 import GpuLoop
+    m = make_model(workdir, "disk18k")
+    for prec in (0, 1):
+        info = GpuLoop(m, precision=prec).plan_info()
+        nt, tiles, blocks = info["nodes_per_tile"], info["node_tiles"], info["node_tile_blocks"]
+        assert tiles == -(-m.num_nodes // nt) and 0 < blocks <= tiles
+        assert nt == 256 or tiles % blocks == 0 or tiles % blocks > 0.9 * blocks
