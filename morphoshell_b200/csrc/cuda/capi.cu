@@ -282,7 +282,7 @@ bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, con
     const int C = L.tile_chunk[K];
     L.C = C;
     // Node sections: for each chunk, runs (node in tile, end) and entries
-    // (slot * 6 + patch slot).  Nodes go in ascending order and each node's
+    // (patch slot * 3 kTile + slot in chunk).  Nodes go in ascending order and each node's
     // entries in ascending t, so a node's entries within a chunk are one run.
     L.run_node.assign(C, {});
     L.run_end.assign(C, {});
@@ -308,7 +308,7 @@ bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, con
                     L.run_end[c].push_back(L.run_end[c].empty() ? 0 : L.run_end[c].back());
                     run_last[c] = j;
                 }
-                L.cent[c].push_back((unsigned short)((li % kTile) * 6 + slot));
+                L.cent[c].push_back((unsigned short)(slot * 3 * kTile + li % kTile));
                 L.run_end[c].back() += 1;
             }
         }
@@ -328,7 +328,8 @@ bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, con
             for (size_t r = 0; ok && r < R; ++r)
                 ok = L.run_node[c][r] < NT && L.run_end[c][r] > (r ? L.run_end[c][r - 1] : 0);
             ok = ok && (R == 0 ? E == 0 : L.run_end[c][R - 1] == E);
-            for (size_t e = 0; ok && e < E; ++e) ok = L.cent[c][e] < 6 * ntri;
+            for (size_t e = 0; ok && e < E; ++e)
+                ok = L.cent[c][e] / (3 * kTile) < 6 && L.cent[c][e] % (3 * kTile) < ntri;
             if (!ok) {
                 err = "node tile chunk fails its bounds";
                 return false;

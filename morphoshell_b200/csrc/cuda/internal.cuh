@@ -138,7 +138,9 @@ constexpr int kTile = 128;
 //   int32 header {R, E, ntri, 0}
 //   uint16 run_node[R]   node (index in the tile) of each run
 //   uint16 run_end[R]    end of the run's entries (exclusive, cumulative)
-//   uint16 ent[E]        (slot in chunk) * 6 + patch slot, per node ascending t
+//   uint16 ent[E]        patch slot * 3 kTile + slot in chunk, per node ascending t
+//                        (the x component of the contribution in the block's
+//                        field-major staging area; y and z follow kTile apart)
 // A block sums a node's contributions run by run, chunk by chunk, so every
 // node's force is the sum in ascending triangle order, as in the node kernel.
 struct NodeTilePlan {

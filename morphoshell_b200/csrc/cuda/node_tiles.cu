@@ -3,25 +3,26 @@
 //
 // A persistent block walks node tiles (blockIdx.x, then every gridDim.x-th).
 // For each tile it streams the chunk records of the tile's triangle list
-// (every triangle whose patch touches one of the tile's nodes, ascending t):
-// thread 0 copies the next record into the other half of a shared-memory
-// double buffer with one cp.async.bulk (completion counted in bytes on an
-// mbarrier; the next tile's first record follows the current tile's last),
-// while the block computes the current chunk.  Each thread computes one
-// triangle's 18 contributions (the arithmetic of the bulk-copy per-triangle
-// kernel, tile_tri), stages them in the consumed weight area, and then the
-// chunk's runs add them to the tile's per-node accumulators in shared
-// memory: one thread per run, a run being one node's entries in this chunk in
-// ascending triangle order.  Chunks are taken in order, so each node's force
-// is summed in ascending triangle order from zero -- the order, and so the
-// bits, of the node kernel's gather (calc_deformation_forces.cpp:185).  After
-// the tile's last chunk the block finishes its nodes (damping, constraints,
+// (every triangle whose patch touches one of the tile's nodes, ascending t).
+// Thread 0 copies a record with two cp.async.bulk (the tables into the
+// block's single table area, the node section into one of two slots;
+// completion counted in bytes on one mbarrier).  The copy of the next record
+// starts as soon as every thread holds its triangle's tables in registers,
+// so it lands while the block computes: each thread forms one triangle's 18
+// contributions (the arithmetic of the bulk-copy per-triangle kernel,
+// tile_tri) and stages them in a field-major area, and then the chunk's runs
+// add them to the tile's per-node accumulators in shared memory: one thread
+// per run, a run being one node's entries in this chunk in ascending
+// triangle order.  Chunks are taken in order, so each node's force is summed
+// in ascending triangle order from zero -- the order, and so the bits, of
+// the node kernel's gather (calc_deformation_forces.cpp:185).  After the
+// tile's last chunk the block finishes its nodes (damping, constraints,
 // guard, equilibrium maxima, symplectic Euler; node_core) and moves on.
 //
 // Cost against the two-kernel step: triangles on tile borders are computed
-// once per tile they touch (16-20 % more triangle work at 1024-node tiles),
-// but the contribution round trip through HBM (144 B per triangle in FP64,
-// 72 B mixed) and the node kernel's incidence lists disappear.
+// once per tile they touch (about 20 % more triangle work at 700-node
+// tiles), but the contribution round trip through HBM (144 B per triangle in
+// FP64, 72 B mixed) and the node kernel's incidence lists disappear.
 #include <algorithm>
 #include <climits>
 
@@ -49,7 +50,7 @@ constexpr int kFinishBatch = 1;
 template <bool MIXED>
 struct NtSmem {
     static constexpr size_t fixed = TileLayout<MIXED>::bytes;
-    static constexpr size_t stage = (size_t)kTile * contrib_stride<MIXED>() * (MIXED ? 4 : 8);
+    static constexpr size_t stage = (size_t)kTile * 18 * (MIXED ? 4 : 8);
     __host__ __device__ static size_t ns_cap(size_t stride) { return stride - fixed; }
     __host__ __device__ static size_t bytes(size_t stride, int nodes) {
         return fixed + stage + 2 * ns_cap(stride) + 24 * (size_t)nodes;
@@ -71,8 +72,6 @@ __global__ void __launch_bounds__(kTile, MIXED ? MSB_NT_MINB_MIXED : MSB_NT_MINB
     using R = typename Real<MIXED>::T;
     using L = TileLayout<MIXED>;
     using SM = NtSmem<MIXED>;
-    constexpr int CS = contrib_stride<MIXED>();
-    constexpr int S = contrib_slot<MIXED>();
     const int gstep = global_step(s.err, sc.step);
     if (stale(s.err, gstep)) return;  // uniform over the grid
     double dial = 0.0, lam = 0.0, pw = 0.0;
@@ -128,6 +127,8 @@ __global__ void __launch_bounds__(kTile, MIXED ? MSB_NT_MINB_MIXED : MSB_NT_MINB
         const int cend = __ldg(q.tile_chunk + tile + 1);
         const int ntile = tile + gridDim.x;
         const int cn = ntile < q.ntiles ? __ldg(q.tile_chunk + ntile) : -1;
+        const int n0 = tile * q.nodes;
+        const int nn = min(q.nodes, m.N - n0);
         for (; c < cend; ++c) {
             const int nc = c + 1 < cend ? c + 1 : cn;
             // This barrier also ends the previous chunk's runs, so the
@@ -154,7 +155,9 @@ __global__ void __launch_bounds__(kTile, MIXED ? MSB_NT_MINB_MIXED : MSB_NT_MINB
             const double area = saux[i], c2 = saux[kTile + i], s2 = saux[2 * kTile + i], cs = saux[3 * kTile + i];
             const bool live = i < hd.z;
             const int t = (need_t && live) ? __ldg(q.chunk_tri + (size_t)c * kTile + i) : 0;
-            // Order these reads before the bulk copy that refills the area.
+            // The table loads above may still be in flight (their values are
+            // used after the barrier): order them before the bulk copy that
+            // refills the area.
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncthreads();
             if (i == 0 && nc >= 0) fetch(nc, slot ^ 1);
@@ -162,31 +165,34 @@ __global__ void __launch_bounds__(kTile, MIXED ? MSB_NT_MINB_MIXED : MSB_NT_MINB
 #pragma unroll
             for (int j = 0; j < 18; ++j) f[j] = R(0);
             if (live) tile_tri<DIAL, MIXED>(m, p, pos, dial, lam, pw, t, ids, cf, area, c2, s2, cs, f);
-            stage_contrib<MIXED>(stage + i * CS, f);
+#pragma unroll
+            for (int k = 0; k < 18; ++k) stage[k * kTile + i] = f[k];
             __syncthreads();
             // Runs: one node's entries of this chunk each, distinct nodes, so
             // the runs of a chunk add in parallel without conflicts.
-            const unsigned short* rn = reinterpret_cast<const unsigned short*>(ns + 16);
-            const unsigned short* re = rn + hd.x;
-            const unsigned short* en = re + hd.x;
-            for (int r = i; r < hd.x; r += kTile) {
-                const int j = rn[r];
-                int e = r ? re[r - 1] : 0;
-                const int e1 = re[r];
-                double a0 = acc[3 * j], a1 = acc[3 * j + 1], a2 = acc[3 * j + 2];
-                for (; e < e1; ++e) {
-                    const R* v = stage + S * en[e];
-                    a0 += (double)v[0];
-                    a1 += (double)v[1];
-                    a2 += (double)v[2];
+            {
+                // Staging is field-major: component k of patch slot sl of
+                // the chunk's triangle i at stage[(3 sl + k) kTile + i]; an
+                // entry holds sl * 3 kTile + i.
+                const unsigned short* rn = reinterpret_cast<const unsigned short*>(ns + 16);
+                const unsigned short* re = rn + hd.x;
+                const unsigned short* en = re + hd.x;
+                for (int r = i; r < hd.x; r += kTile) {
+                    const int j = rn[r];
+                    int e = r ? re[r - 1] : 0;
+                    const int e1 = re[r];
+                    double a0 = acc[3 * j], a1 = acc[3 * j + 1], a2 = acc[3 * j + 2];
+                    for (; e < e1; ++e) {
+                        const R* v = stage + en[e];
+                        a0 += (double)v[0];
+                        a1 += (double)v[kTile];
+                        a2 += (double)v[2 * kTile];
+                    }
+                    acc[3 * j] = a0;
+                    acc[3 * j + 1] = a1;
+                    acc[3 * j + 2] = a2;
                 }
-                acc[3 * j] = a0;
-                acc[3 * j + 1] = a1;
-                acc[3 * j + 2] = a2;
             }
-            // Generic reads of this node-section slot come before the copy
-            // that refills it two chunks on.
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             slot ^= 1;
         }
         if (failed) break;
@@ -195,8 +201,6 @@ __global__ void __launch_bounds__(kTile, MIXED ? MSB_NT_MINB_MIXED : MSB_NT_MINB
         // ready for the next tile (whose first runs come after at least two
         // more block barriers).
         __syncthreads();
-        const int n0 = tile * q.nodes;
-        const int nn = min(q.nodes, m.N - n0);
         for (int j0 = 0; j0 < nn; j0 += kTile * kFinishBatch) {
             NodeIn in[kFinishBatch];
 #pragma unroll
