@@ -38,8 +38,8 @@ using namespace stepdev;
 using namespace tridev;
 using namespace tiles;
 
-// Nodes finished per thread with their loads in flight together (more than
-// one spills at the register budget of 3 or 4 blocks per SM).
+// Nodes finished per thread with their loads in flight together (two spill
+// at the register budget of 3 blocks per SM and were measured slower).
 constexpr int kFinishBatch = 1;
 
 // Shared memory of a block: the chunk's fixed part (ids, weights,
