@@ -303,8 +303,10 @@ typedef struct ms_batch_inst_status {
 } ms_batch_inst_status;
 
 /* Launch schedule: threads per block of the per-triangle kernel (0: the
- * persistent kernel fed by bulk-copied 128-triangle tiles, the default) and
- * of the per-node kernel, steps per captured graph (even). */
+ * persistent kernel fed by bulk-copied 128-triangle tiles; -1: the
+ * node-tiled one-kernel step, node_block ignored -- the default when the
+ * union has a node tile for every resident block, else 0) and of the
+ * per-node kernel, steps per captured graph (even). */
 typedef struct ms_batch_schedule {
     int32_t tri_block, node_block, chunk_steps;
 } ms_batch_schedule;

@@ -562,6 +562,8 @@ class Batch:
         return {k: getattr(s, k) for k, _ in s._fields_}
 
     def set_schedule(self, tri_block: int, node_block: int, chunk_steps: int):
+        """tri_block -1: node-tiled one-kernel step (node_block ignored); 0:
+        bulk-copy tile kernel; 64/128/256: per-triangle kernel block size."""
         s = ms_batch_schedule(tri_block, node_block, chunk_steps)
         self._chk(lib().ms_batch_set_schedule(self._h, C.byref(s)), "ms_batch_set_schedule")
 

@@ -29,6 +29,7 @@
 
 #include "../../../include/morphoshell_gpu.h"
 #include "internal.cuh"
+#include "node_tile_walk.cuh"
 #include "step_common.cuh"
 #include "tile_copy.cuh"
 #include "tri_contrib.cuh"
@@ -109,6 +110,39 @@ __global__ void __launch_bounds__(BLOCK) k_batch_tri(const DevMesh m, const Clus
     for (int j = lane; j < total; j += 32) out[j] = sw[j];
 }
 
+// One triangle of a tile or chunk record with its instance's material and
+// protocol-3 values (nothing for a done or failed instance).  Shared by the
+// tile and node-tile kernels, so they give the same bits.
+template <bool MIXED>
+__device__ __forceinline__ void batch_tri(const DevMesh& m, const int* __restrict__ tri_inst,
+                                          const InstParams* __restrict__ ip, const InstState* __restrict__ is,
+                                          const double* __restrict__ pos, int t, const int (&ids)[6],
+                                          const typename Real<MIXED>::T (&c)[24], double area, double c2, double s2,
+                                          double cs, typename Real<MIXED>::T (&f)[18]) {
+    const int inst = __ldg(tri_inst + t);
+    const InstState& st = is[inst];
+    if (is_frozen(st.status)) return;
+    const InstParams& q = ip[inst];
+    TriMat<double> mt;
+    if (q.uniform_hmu) {
+        mt.h = q.h;
+        mt.mu = q.mu;
+    } else {
+        mt.h = __ldg(m.thick + t);
+        mt.mu = __ldg(m.shear + t);
+    }
+    mt.area = area;
+    lce_metric(c2, s2, cs, __dmul_rn(st.cur_lam, st.cur_lam), st.cur_pw, mt);
+    double P[6][3];
+#pragma unroll
+    for (int sl = 0; sl < 6; ++sl) {
+        P[sl][0] = __ldg(pos + ids[sl]);
+        P[sl][1] = __ldg(pos + m.N + ids[sl]);
+        P[sl][2] = __ldg(pos + 2 * m.N + ids[sl]);
+    }
+    tri_forces<MIXED>(P, c, mt, q.nu, q.gamma, f);
+}
+
 // The same contributions from bulk-copied tile records (tile_copy.cuh),
 // persistent blocks; tri_inst[t] is the triangle's instance.
 template <bool MIXED>
@@ -125,53 +159,18 @@ __global__ void __launch_bounds__(kTile) k_batch_tri_tiles(const DevMesh m, cons
     tiles::tile_loop<MIXED>(
         m.T, tl, out, err,
         [&](int t, const int (&ids)[6], const R (&c)[24], double area, double c2, double s2, double cs, R (&f)[18]) {
-            const int inst = __ldg(tri_inst + t);
-            const InstState& st = is[inst];
-            if (is_frozen(st.status)) return;
-            const InstParams& q = ip[inst];
-            TriMat<double> mt;
-            if (q.uniform_hmu) {
-                mt.h = q.h;
-                mt.mu = q.mu;
-            } else {
-                mt.h = __ldg(m.thick + t);
-                mt.mu = __ldg(m.shear + t);
-            }
-            mt.area = area;
-            lce_metric(c2, s2, cs, __dmul_rn(st.cur_lam, st.cur_lam), st.cur_pw, mt);
-            double P[6][3];
-#pragma unroll
-            for (int sl = 0; sl < 6; ++sl) {
-                P[sl][0] = __ldg(pos + ids[sl]);
-                P[sl][1] = __ldg(pos + m.N + ids[sl]);
-                P[sl][2] = __ldg(pos + 2 * m.N + ids[sl]);
-            }
-            tri_forces<MIXED>(P, c, mt, q.nu, q.gamma, f);
+            batch_tri<MIXED>(m, tri_inst, ip, is, pos, t, ids, c, area, c2, s2, cs, f);
         });
 }
 
-template <bool MIXED, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_batch_node(const DevMesh m, const DevState s,
-                                                      const int* __restrict__ node_inst,
-                                                      const InstParams* __restrict__ ip, InstState* __restrict__ is,
-                                                      double* __restrict__ fnorm, double* __restrict__ vnorm,
-                                                      int parity) {
-    const int n = blockIdx.x * BLOCK + threadIdx.x;
+// Everything after the deformation-force sum for node n of a live instance:
+// node_finish with the instance's scalars, |F| and |v| to fnorm / vnorm on
+// the instance's check steps, a guard trip into the instance's guard key.
+__device__ __forceinline__ void batch_node_core(const DevMesh& m, const DevState& s, const InstParams& q,
+                                                InstState* __restrict__ is, int inst, int n, double Fx, double Fy,
+                                                double Fz, double* __restrict__ fnorm, double* __restrict__ vnorm,
+                                                int parity) {
     const int N = m.N;
-    int inst = 0;
-    bool active = false;
-    if (n < N) {
-        inst = __ldg(node_inst + n);
-        active = !is_frozen(is[inst].status);
-    }
-    if (!__any_sync(0xffffffffu, active)) return;  // warp-uniform
-    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
-    if constexpr (MIXED) gather_sell<float>(m, m.contrib_f, n, Fx, Fy, Fz);
-    else gather_sell<double>(m, s.contrib, n, Fx, Fy, Fz);
-    if (!active) return;
-    // Damping, constraints, |F| and |v|, guard, update: node_finish with
-    // the instance's scalars.
-    const InstParams& q = ip[inst];
     const double damping = is[inst].damping;
     const int check = is[inst].check_now;
     const double* pos = pos_buf(s, parity);
@@ -202,6 +201,56 @@ __global__ void __launch_bounds__(BLOCK) k_batch_node(const DevMesh m, const Dev
     nvel[n] = nvx;
     nvel[N + n] = nvy;
     nvel[2 * N + n] = nvz;
+}
+
+template <bool MIXED, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_batch_node(const DevMesh m, const DevState s,
+                                                      const int* __restrict__ node_inst,
+                                                      const InstParams* __restrict__ ip, InstState* __restrict__ is,
+                                                      double* __restrict__ fnorm, double* __restrict__ vnorm,
+                                                      int parity) {
+    const int n = blockIdx.x * BLOCK + threadIdx.x;
+    const int N = m.N;
+    int inst = 0;
+    bool active = false;
+    if (n < N) {
+        inst = __ldg(node_inst + n);
+        active = !is_frozen(is[inst].status);
+    }
+    if (!__any_sync(0xffffffffu, active)) return;  // warp-uniform
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    if constexpr (MIXED) gather_sell<float>(m, m.contrib_f, n, Fx, Fy, Fz);
+    else gather_sell<double>(m, s.contrib, n, Fx, Fy, Fz);
+    if (!active) return;
+    batch_node_core(m, s, ip[inst], is, inst, n, Fx, Fy, Fz, fnorm, vnorm, parity);
+}
+
+// The whole step of the union in one kernel (node_tile_walk.cuh): a block
+// sums the forces of its tiles of nodes in shared memory, computing every
+// triangle that touches them, and updates the tiles' live nodes.
+#ifndef MSB_NT_MINB
+#define MSB_NT_MINB 3
+#endif
+#ifndef MSB_NT_MINB_MIXED
+#define MSB_NT_MINB_MIXED 4
+#endif
+template <bool MIXED>
+__global__ void __launch_bounds__(kTile, MIXED ? MSB_NT_MINB_MIXED : MSB_NT_MINB)
+    k_batch_node_tiles(const DevMesh m, const NodeTilePlan q, const DevState s, const int* __restrict__ tri_inst,
+                       const int* __restrict__ node_inst, const InstParams* __restrict__ ip,
+                       InstState* __restrict__ is, double* __restrict__ fnorm, double* __restrict__ vnorm, int* err,
+                       int parity) {
+    using R = typename Real<MIXED>::T;
+    const double* pos = pos_buf(s, parity);
+    tiles::node_tile_walk<MIXED>(
+        q, m.N, true, err,
+        [&](int t, const int (&ids)[6], const R (&c)[24], double area, double c2, double s2, double cs, R (&f)[18]) {
+            batch_tri<MIXED>(m, tri_inst, ip, is, pos, t, ids, c, area, c2, s2, cs, f);
+        },
+        [&](int n, double Fx, double Fy, double Fz) {
+            const int inst = __ldg(node_inst + n);
+            if (!is_frozen(is[inst].status)) batch_node_core(m, s, ip[inst], is, inst, n, Fx, Fy, Fz, fnorm, vnorm, parity);
+        });
 }
 
 constexpr int kPostBlock = 256;
@@ -270,9 +319,11 @@ __global__ void __launch_bounds__(kPostBlock) k_batch_post(const InstParams* __r
 struct Sched {
     int tri_block, node_block;
 };
-// tri_block 0: the persistent bulk-copy tile kernel.
-constexpr Sched kScheds[] = {{0, 256},   {128, 256}, {64, 256}, {256, 256}, {128, 128},
-                             {64, 128},  {256, 128}, {128, 512}, {0, 128}};
+// tri_block -1: the node-tiled one-kernel step (node_block unused); 0: the
+// persistent bulk-copy tile kernel.
+constexpr int kSchedNodeTiles = 0, kSchedTiles = 1, kSchedAos = 2;
+constexpr Sched kScheds[] = {{-1, 0},    {0, 256},   {128, 256}, {64, 256}, {256, 256},
+                             {128, 128}, {64, 128},  {256, 128}, {128, 512}, {0, 128}};
 constexpr int kNumScheds = sizeof(kScheds) / sizeof(kScheds[0]);
 
 template <bool MIXED>
@@ -338,8 +389,10 @@ struct ms_batch {
     double* d_vnorm = nullptr;
     InstState* h_is = nullptr;  // pinned mirror
     int* d_tri_inst = nullptr;   // [T]
-    int* d_err = nullptr;        // copy-wait timeouts of the tile kernel
+    int* d_err = nullptr;        // copy-wait timeouts of the tile kernels
     int tile_grid = 0;           // 0: tile kernel unavailable
+    NodeTilePlan ntp{};          // node-tiled step over the union
+    bool have_nt = false;
     int parity = 0;
     int sched = 0;
     int chunk = 64;
@@ -401,7 +454,19 @@ ms_status launch_step(ms_batch* b, int parity, int sched) {
     const int n = b->n_inst;
     k_batch_pre<<<(n + 127) / 128, 128, 0, st>>>(b->d_ip, b->d_is, n);
     cudaError_t e;
-    if (sc.tri_block == 0) {
+    if (sc.tri_block < 0) {
+        const NodeTilePlan& q = b->ntp;
+        const int grid = std::min(q.ntiles, q.grid);
+        if (b->precision == MS_PRECISION_MIXED)
+            k_batch_node_tiles<true><<<grid, kTile, tiles::NtSmem<true>::bytes(q.stride, q.nodes), st>>>(
+                b->m, q, b->s, b->d_tri_inst, b->d_node_inst, b->d_ip, b->d_is, b->d_fnorm, b->d_vnorm, b->d_err,
+                parity);
+        else
+            k_batch_node_tiles<false><<<grid, kTile, tiles::NtSmem<false>::bytes(q.stride, q.nodes), st>>>(
+                b->m, q, b->s, b->d_tri_inst, b->d_node_inst, b->d_ip, b->d_is, b->d_fnorm, b->d_vnorm, b->d_err,
+                parity);
+        e = cudaGetLastError();
+    } else if (sc.tri_block == 0) {
         const int ntiles = (b->m.T + kTile - 1) / kTile;
         const int grid = std::min(ntiles, b->tile_grid);
         if (b->precision == MS_PRECISION_MIXED)
@@ -701,7 +766,6 @@ ms_status ms_batch_create(const ms_batch_instance* inst, int32_t n, int32_t devi
             const long long ntiles = (T + kTile - 1) / kTile;
             std::vector<unsigned char> buf(rec * ntiles, 0);
             const size_t ids_b = 6 * kTile * 4, coef_b = 24 * kTile * (mixed ? 4 : 8);
-            std::vector<int> tri_inst(T);
             for (long long t = 0; t < T; ++t) {
                 const long long tile = t / kTile, li = t % kTile;
                 unsigned char* r = buf.data() + rec * tile;
@@ -716,13 +780,9 @@ ms_status ms_batch_create(const ms_batch_instance* inst, int32_t n, int32_t devi
                     for (int k = 0; k < 24; ++k) c[k * kTile + li] = coef[24ULL * t + k];
                 }
                 for (int k = 0; k < 4; ++k) ax[k * kTile + li] = aux[4ULL * t + k];
-                tri_inst[t] = idx[8ULL * t + 7];
             }
             unsigned char* d_tiles;
-            if ((st = bupload(b, &d_tiles, buf)) || (st = bupload(b, &b->d_tri_inst, tri_inst)) ||
-                (st = balloc(b, &b->d_err, 1)))
-                return bail(st);
-            if (cudaMemset(b->d_err, 0, sizeof(int)) != cudaSuccess) return bail(MS_ERR_CUDA);
+            if ((st = bupload(b, &d_tiles, buf))) return bail(st);
             if (mixed) p.tiles_f = d_tiles;
             else p.tiles = d_tiles;
             int dev = 0, sms = 0;
@@ -733,7 +793,73 @@ ms_status ms_batch_create(const ms_batch_instance* inst, int32_t n, int32_t devi
             cudaGetLastError();
             b->tile_grid = 0;
         }
-        b->sched = b->tile_grid > 0 ? 0 : 1;
+    }
+    {
+        std::vector<int> tri_inst(T);
+        for (long long t = 0; t < T; ++t) tri_inst[t] = idx[8ULL * t + 7];
+        if ((st = bupload(b, &b->d_tri_inst, tri_inst)) || (st = balloc(b, &b->d_err, 1))) return bail(st);
+        if (cudaMemset(b->d_err, 0, sizeof(int)) != cudaSuccess) return bail(MS_ERR_CUDA);
+    }
+    // Node-tiled one-kernel step over the union (node_tile_plan.cu).
+    {
+        const int mixed = precision == MS_PRECISION_MIXED;
+        std::vector<int> patch6(6ULL * T);
+        for (long long t = 0; t < T; ++t)
+            for (int k = 0; k < 6; ++k) patch6[6ULL * t + k] = idx[8ULL * t + k];
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        auto blocks_for = [&](size_t smem) {
+            int nb_ = 0;
+            cudaError_t ea = mixed ? cudaFuncSetAttribute(k_batch_node_tiles<true>,
+                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                                   : cudaFuncSetAttribute(k_batch_node_tiles<false>,
+                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (ea == cudaSuccess)
+                ea = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_, k_batch_node_tiles<true>, kTile, smem)
+                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_, k_batch_node_tiles<false>, kTile,
+                                                                           smem);
+            if (ea != cudaSuccess) {
+                cudaGetLastError();
+                nb_ = 0;
+            }
+            return nb_;
+        };
+        NodeTileLayout L;
+        std::string err;
+        int NT = 0, blocks = 0;
+        if (!choose_node_tiles(patch6.data(), (int)N, (int)T, mixed, sms, mixed ? MSB_NT_MINB_MIXED : MSB_NT_MINB,
+                               mixed ? 1008 : 928, 256, off, ent, blocks_for, L, NT, blocks, err))
+            return bail(bfail(b, MS_ERR_INVALID_ARGUMENT, err));
+        if (blocks > 0) {
+            std::vector<unsigned char> rec;
+            std::vector<int> ctri;
+            fill_node_tile_records(L, patch6.data(), mixed ? nullptr : coef.data(), mixed ? mcoef.data() : nullptr,
+                                   nullptr, aux.data(), mixed, rec, ctri);
+            unsigned char* d_rec;
+            int *d_tc, *d_ctri;
+            unsigned* d_bytes;
+            if ((st = bupload(b, &d_rec, rec)) || (st = bupload(b, &d_tc, L.tile_chunk)) ||
+                (st = bupload(b, &d_bytes, L.bytes)) || (st = bupload(b, &d_ctri, ctri)))
+                return bail(st);
+            NodeTilePlan& q = b->ntp;
+            q.nodes = NT;
+            q.ntiles = L.K;
+            q.nchunks = L.C;
+            q.grid = sms * blocks;
+            q.stride = L.stride;
+            q.rec = d_rec;
+            q.tile_chunk = d_tc;
+            q.chunk_bytes = d_bytes;
+            q.chunk_tri = d_ctri;
+            b->have_nt = true;
+        }
+        // The one-kernel step once every block has a tile of its own
+        // (measured fastest on B200 for the single-mesh step), else the
+        // tile kernel, else the per-triangle kernel.
+        b->sched = (b->have_nt && b->ntp.ntiles >= b->ntp.grid) ? kSchedNodeTiles
+                   : b->tile_grid > 0                         ? kSchedTiles
+                                                              : kSchedAos;
     }
     m.mass = d_mass;
     m.fixed = d_fixed;
@@ -875,8 +1001,9 @@ ms_status ms_batch_set_schedule(ms_batch* b, const ms_batch_schedule* s) {
     if (s->chunk_steps <= 0 || s->chunk_steps % 2 || s->chunk_steps > 1024)
         return bfail(b, MS_ERR_INVALID_ARGUMENT, "chunk_steps must be even, 2..1024");
     for (int k = 0; k < kNumScheds; ++k)
-        if (kScheds[k].tri_block == s->tri_block && kScheds[k].node_block == s->node_block &&
-            (s->tri_block != 0 || b->tile_grid > 0)) {
+        if (kScheds[k].tri_block == s->tri_block &&
+            (kScheds[k].node_block == s->node_block || s->tri_block < 0) && (s->tri_block != 0 || b->tile_grid > 0) &&
+            (s->tri_block >= 0 || b->have_nt)) {
             b->sched = k;
             b->chunk = s->chunk_steps;
             return MS_OK;
@@ -938,6 +1065,7 @@ ms_status ms_batch_autotune(ms_batch* b, int32_t steps, ms_batch_schedule* chose
     if (copy_state(true) != cudaSuccess) rc = bcuda(b, cudaGetLastError(), "autotune save");
     for (int k = 0; k < kNumScheds && rc == MS_OK; ++k) {
         if (kScheds[k].tri_block == 0 && b->tile_grid == 0) continue;
+        if (kScheds[k].tri_block < 0 && !b->have_nt) continue;
         // one untimed pass (graph instantiation, caches), then the timed one
         for (int rep = 0; rep < 2 && rc == MS_OK; ++rep) {
             if (copy_state(false) != cudaSuccess) {

@@ -227,122 +227,6 @@ ms_status build_tiles(ms_handle* h, const ms_mesh_desc* d) {
     return MS_OK;
 }
 
-// Host-side layout of the node-tiled step (NodeTilePlan) for tiles of NT
-// consecutive nodes: every tile's triangle list (ascending t), its chunks and
-// their node sections, checked against the bounds the kernel relies on.
-struct NodeTileLayout {
-    int K = 0, C = 0;
-    std::vector<long long> start;   // [K + 1] list offsets into lst
-    std::vector<int> lst;           // triangle lists, tile after tile
-    std::vector<int> tile_chunk;    // [K + 1]
-    std::vector<std::vector<unsigned short>> run_node, run_end, cent;  // per chunk
-    std::vector<unsigned> bytes;    // [C] bytes to copy (fixed part + node section)
-    size_t fixed = 0, stride = 0, ns_max = 0;
-};
-
-bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, const std::vector<int>& off,
-                      const std::vector<int>& ent, NodeTileLayout& L, std::string& err) {
-    if (NT <= 0 || NT > 65536) {
-        err = "nodes per tile must be in 1..65536";
-        return false;
-    }
-    const int K = (N + NT - 1) / NT;
-    L.K = K;
-    L.start.assign(K + 1, 0);
-    auto tiles_of = [&](int t, int* out) {
-        int n = 0;
-        for (int k = 0; k < 6; ++k) {
-            const int tk = patch_ids[6LL * t + k] / NT;
-            bool seen = false;
-            for (int j = 0; j < n; ++j) seen = seen || out[j] == tk;
-            if (!seen) out[n++] = tk;
-        }
-        return n;
-    };
-    int tk[6];
-    for (int t = 0; t < T; ++t) {
-        const int n = tiles_of(t, tk);
-        for (int j = 0; j < n; ++j) L.start[tk[j] + 1] += 1;
-    }
-    for (int k = 0; k < K; ++k) L.start[k + 1] += L.start[k];
-    L.lst.assign(L.start[K], 0);
-    {
-        std::vector<long long> fill(L.start.begin(), L.start.end() - 1);
-        for (int t = 0; t < T; ++t) {
-            const int n = tiles_of(t, tk);
-            for (int j = 0; j < n; ++j) L.lst[fill[tk[j]]++] = t;
-        }
-    }
-    L.tile_chunk.assign(K + 1, 0);
-    // At least one chunk per tile (an empty one for a tile of isolated
-    // nodes), so that every tile's walk starts with a copy of its own record.
-    for (int k = 0; k < K; ++k)
-        L.tile_chunk[k + 1] =
-            L.tile_chunk[k] + std::max(1, (int)((L.start[k + 1] - L.start[k] + kTile - 1) / kTile));
-    const int C = L.tile_chunk[K];
-    L.C = C;
-    // Node sections: for each chunk, runs (node in tile, end) and entries
-    // (patch slot * 3 kTile + slot in chunk).  Nodes go in ascending order and each node's
-    // entries in ascending t, so a node's entries within a chunk are one run.
-    L.run_node.assign(C, {});
-    L.run_end.assign(C, {});
-    L.cent.assign(C, {});
-    std::vector<int> run_last(C, -1);
-    for (int k = 0; k < K; ++k) {
-        const int* L0 = L.lst.data() + L.start[k];
-        const int* L1 = L.lst.data() + L.start[k + 1];
-        for (int n = k * NT; n < std::min(N, (k + 1) * NT); ++n) {
-            int last_t = -1;
-            for (int e = off[n]; e < off[n + 1]; ++e) {
-                const int t = ent[e] / 6, slot = ent[e] % 6;
-                const int li = (int)(std::lower_bound(L0, L1, t) - L0);
-                if (L0 + li == L1 || L0[li] != t || t < last_t) {
-                    err = "incidence lists disagree with the patches";
-                    return false;
-                }
-                last_t = t;
-                const int c = L.tile_chunk[k] + li / kTile;
-                const int j = n - k * NT;
-                if (run_last[c] != j) {
-                    L.run_node[c].push_back((unsigned short)j);
-                    L.run_end[c].push_back(L.run_end[c].empty() ? 0 : L.run_end[c].back());
-                    run_last[c] = j;
-                }
-                L.cent[c].push_back((unsigned short)(slot * 3 * kTile + li % kTile));
-                L.run_end[c].back() += 1;
-            }
-        }
-    }
-    L.fixed = tile_record_bytes(mixed);
-    L.ns_max = 16;
-    L.bytes.assign(C, 0);
-    for (int k = 0; k < K; ++k) {
-        for (int c = L.tile_chunk[k]; c < L.tile_chunk[k + 1]; ++c) {
-            const long long first = L.start[k] + (long long)(c - L.tile_chunk[k]) * kTile;
-            const int ntri = (int)std::max<long long>(0, std::min<long long>(kTile, L.start[k + 1] - first));
-            const size_t R = L.run_node[c].size(), E = L.cent[c].size();
-            // What the kernel indexes: entries inside the chunk's live slots,
-            // run nodes inside the tile's accumulators, run ends ascending up
-            // to E, everything inside one record.
-            bool ok = R <= 6 * kTile && E <= 6 * kTile;
-            for (size_t r = 0; ok && r < R; ++r)
-                ok = L.run_node[c][r] < NT && L.run_end[c][r] > (r ? L.run_end[c][r - 1] : 0);
-            ok = ok && (R == 0 ? E == 0 : L.run_end[c][R - 1] == E);
-            for (size_t e = 0; ok && e < E; ++e)
-                ok = L.cent[c][e] / (3 * kTile) < 6 && L.cent[c][e] % (3 * kTile) < ntri;
-            if (!ok) {
-                err = "node tile chunk fails its bounds";
-                return false;
-            }
-            const size_t ns = (16 + 4 * R + 2 * E + 15) / 16 * 16;
-            L.ns_max = std::max(L.ns_max, ns);
-            L.bytes[c] = (unsigned)(L.fixed + ns);
-        }
-    }
-    L.stride = L.fixed + (L.ns_max + 127) / 128 * 128;
-    return true;
-}
-
 // Largest nodes per tile of the node-tiled step: the largest tiles (fewest
 // border triangles computed twice) whose blocks still fit 3 (FP64) or 4
 // (mixed) to an SM; and the smallest tiles worth their border.
@@ -369,71 +253,30 @@ ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vecto
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int target = node_tile_blocks_target(mixed);
-    int nt_max = mixed ? MSB_NT_NODES_MIXED : MSB_NT_NODES;
     NodeTileLayout L;
     std::string err;
     int NT = 0, blocks = 0;
-    size_t smem = 0;
-    for (int attempt = 0; attempt < 4; ++attempt) {
-        const long long slots = (long long)std::max(sms, 1) * target;
-        const long long k = std::max(1LL, (N + slots * nt_max - 1) / (slots * nt_max));
-        NT = std::max(std::min(nt_max, kNtNodesMin), (int)((N + k * slots - 1) / (k * slots)));
-        L = NodeTileLayout();
-        if (!node_tile_layout(d->patch_ids, N, T, NT, mixed, off, ent, L, err))
-            return fail(h, MS_ERR_INVALID_ARGUMENT, err);
-        smem = node_tile_smem(L.stride, NT, mixed);
-        blocks = 0;
-        if (smem > 227 * 1024 || prepare_node_tile_kernels(mixed, smem, &blocks) != cudaSuccess) {
+    auto blocks_for = [&](size_t smem) {
+        int b = 0;
+        if (prepare_node_tile_kernels(mixed, smem, &b) != cudaSuccess) {
             cudaGetLastError();
-            blocks = 0;
+            b = 0;
         }
-        if (blocks >= target) break;
-        nt_max = nt_max * 7 / 8;
-    }
+        return b;
+    };
+    if (!choose_node_tiles(d->patch_ids, N, T, mixed, sms, node_tile_blocks_target(mixed),
+                           mixed ? MSB_NT_NODES_MIXED : MSB_NT_NODES, kNtNodesMin, off, ent, blocks_for, L, NT, blocks,
+                           err))
+        return fail(h, MS_ERR_INVALID_ARGUMENT, err);
     if (blocks <= 0) {
         h->have_ntiles = false;
         return MS_OK;  // the other paths remain
     }
     const int K = L.K, C = L.C;
-    const size_t stride = L.stride, fixed = L.fixed;
-    std::vector<unsigned char> buf(stride * C, 0);
+    const size_t stride = L.stride;
+    std::vector<unsigned char> buf;
     std::vector<int>& ctri = h->nt_chunk_tri;
-    ctri.assign((size_t)C * kTile, -1);
-    const size_t ids_b = 6 * kTile * 4, coef_b = 24 * kTile * (mixed ? 4 : 8);
-    for (int k = 0; k < K; ++k) {
-        for (int c = L.tile_chunk[k]; c < L.tile_chunk[k + 1]; ++c) {
-            unsigned char* r = buf.data() + stride * c;
-            int32_t* ids = reinterpret_cast<int32_t*>(r);
-            double* aux = reinterpret_cast<double*>(r + ids_b + coef_b);
-            const long long first = L.start[k] + (long long)(c - L.tile_chunk[k]) * kTile;
-            const int ntri = (int)std::max<long long>(0, std::min<long long>(kTile, L.start[k + 1] - first));
-            for (int i = 0; i < ntri; ++i) {
-                const int t = L.lst[first + i];
-                ctri[(size_t)c * kTile + i] = t;
-                for (int q = 0; q < 6; ++q) ids[q * kTile + i] = d->patch_ids[6LL * t + q];
-                const double* w = d->deriv_coeffs + 24LL * t;
-                if (mixed) {
-                    float* cf = reinterpret_cast<float*>(r + ids_b);
-                    for (int q = 0; q < 24; ++q) cf[q * kTile + i] = (float)w[q];
-                } else {
-                    double* cf = reinterpret_cast<double*>(r + ids_b);
-                    for (int q = 0; q < 24; ++q) cf[q * kTile + i] = w[q];
-                }
-                aux[i] = d->ref_area[t];
-                aux[kTile + i] = 1.0;
-            }
-            int32_t* hd = reinterpret_cast<int32_t*>(r + fixed);
-            const int R = (int)L.run_node[c].size(), E = (int)L.cent[c].size();
-            hd[0] = R;
-            hd[1] = E;
-            hd[2] = ntri;
-            unsigned short* u = reinterpret_cast<unsigned short*>(r + fixed + 16);
-            std::copy(L.run_node[c].begin(), L.run_node[c].end(), u);
-            std::copy(L.run_end[c].begin(), L.run_end[c].end(), u + R);
-            std::copy(L.cent[c].begin(), L.cent[c].end(), u + 2 * R);
-        }
-    }
+    fill_node_tile_records(L, d->patch_ids, d->deriv_coeffs, nullptr, d->ref_area, nullptr, mixed, buf, ctri);
     unsigned char* d_rec;
     int *d_tile_chunk, *d_ctri;
     unsigned* d_bytes;

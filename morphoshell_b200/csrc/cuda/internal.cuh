@@ -21,6 +21,8 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
+#include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -154,9 +156,42 @@ struct NodeTilePlan {
     const unsigned* chunk_bytes;     // [nchunks] bytes to copy of each record (multiple of 16)
     const int* chunk_tri;            // [nchunks][kTile] triangle of each slot, -1 past the chunk's end
 };
-// Largest node section a chunk record may carry: header, runs and entries of
-// kTile triangles with all 6 slots on the tile.
-constexpr int kNodeSectionMax = 16 + 4 * 6 * kTile + 2 * 6 * kTile;
+
+// Host-side layout of a node-tile plan for tiles of NT consecutive nodes
+// (node_tile_plan.cu): every tile's triangle list (ascending t), its chunks
+// and their node sections, each chunk checked against the bounds the kernels
+// rely on (entries inside the chunk's live slots, run nodes inside the tile,
+// run ends ascending, everything inside one record).
+struct NodeTileLayout {
+    int K = 0, C = 0;
+    std::vector<long long> start;   // [K + 1] list offsets into lst
+    std::vector<int> lst;           // triangle lists, tile after tile
+    std::vector<int> tile_chunk;    // [K + 1]
+    std::vector<std::vector<unsigned short>> run_node, run_end, cent;  // per chunk
+    std::vector<unsigned> bytes;    // [C] bytes to copy (fixed part + node section)
+    size_t fixed = 0, stride = 0, ns_max = 0;
+};
+// off/ent: each node's (6t + slot) entries in ascending order (CSR).
+bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, const std::vector<int>& off,
+                      const std::vector<int>& ent, NodeTileLayout& L, std::string& err);
+// A block walks its tiles in turn, so a step takes as long as the block with
+// the most tiles: the tile size is chosen (between nt_min and nt_max nodes)
+// so that the tile count is a multiple of sms x target blocks, at the largest
+// size whose blocks still reach `target` per SM; blocks_for(shared bytes)
+// sets up the kernel and returns its resident blocks per SM (0 when it
+// cannot run).  On return `blocks` is the resident blocks of the chosen plan
+// (0: the kernel cannot run); false with err for inconsistent lists.
+bool choose_node_tiles(const int* patch_ids, int N, int T, int mixed, int sms, int target, int nt_max, int nt_min,
+                       const std::vector<int>& off, const std::vector<int>& ent,
+                       const std::function<int(size_t)>& blocks_for, NodeTileLayout& L, int& NT, int& blocks,
+                       std::string& err);
+// The chunk records of a layout (ids from patch_ids [T][6]; weights from
+// coef_d [T][24] double, or coef_f float for the mixed path when given; the
+// trigonometry block from aux4 [T][4] = area, cos^2, sin^2, cos sin, or
+// when null area with cos^2 = 1) and the triangle of every slot.
+void fill_node_tile_records(const NodeTileLayout& L, const int* patch_ids, const double* coef_d, const float* coef_f,
+                            const double* area, const double* aux4, int mixed, std::vector<unsigned char>& buf,
+                            std::vector<int>& chunk_tri);
 
 // Layout of the per-(triangle, slot) force contributions: x, y, z doubles;
 // for the mixed path x, y, z floats, optionally padded with a zero to 16

@@ -1,0 +1,181 @@
+// Host side of the node-tiled step (node_tiles.cu, the batched variant in
+// batch.cu): the layout of a plan (every tile's triangle list, its chunks and
+// their node sections, checked against every bound the kernels rely on),
+// the choice of tile size, and the chunk records themselves.
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace msb {
+
+bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, const std::vector<int>& off,
+                      const std::vector<int>& ent, NodeTileLayout& L, std::string& err) {
+    if (NT <= 0 || NT > 65536) {
+        err = "nodes per tile must be in 1..65536";
+        return false;
+    }
+    const int K = (N + NT - 1) / NT;
+    L.K = K;
+    L.start.assign(K + 1, 0);
+    auto tiles_of = [&](int t, int* out) {
+        int n = 0;
+        for (int k = 0; k < 6; ++k) {
+            const int tk = patch_ids[6LL * t + k] / NT;
+            bool seen = false;
+            for (int j = 0; j < n; ++j) seen = seen || out[j] == tk;
+            if (!seen) out[n++] = tk;
+        }
+        return n;
+    };
+    int tk[6];
+    for (int t = 0; t < T; ++t) {
+        const int n = tiles_of(t, tk);
+        for (int j = 0; j < n; ++j) L.start[tk[j] + 1] += 1;
+    }
+    for (int k = 0; k < K; ++k) L.start[k + 1] += L.start[k];
+    L.lst.assign(L.start[K], 0);
+    {
+        std::vector<long long> fill(L.start.begin(), L.start.end() - 1);
+        for (int t = 0; t < T; ++t) {
+            const int n = tiles_of(t, tk);
+            for (int j = 0; j < n; ++j) L.lst[fill[tk[j]]++] = t;
+        }
+    }
+    L.tile_chunk.assign(K + 1, 0);
+    // At least one chunk per tile (an empty one for a tile of isolated
+    // nodes), so that every tile's walk starts with a copy of its own record.
+    for (int k = 0; k < K; ++k)
+        L.tile_chunk[k + 1] =
+            L.tile_chunk[k] + std::max(1, (int)((L.start[k + 1] - L.start[k] + kTile - 1) / kTile));
+    const int C = L.tile_chunk[K];
+    L.C = C;
+    // Node sections: for each chunk, runs (node in tile, end) and entries
+    // (patch slot * 3 kTile + slot in chunk).  Nodes go in ascending order and each node's
+    // entries in ascending t, so a node's entries within a chunk are one run.
+    L.run_node.assign(C, {});
+    L.run_end.assign(C, {});
+    L.cent.assign(C, {});
+    std::vector<int> run_last(C, -1);
+    for (int k = 0; k < K; ++k) {
+        const int* L0 = L.lst.data() + L.start[k];
+        const int* L1 = L.lst.data() + L.start[k + 1];
+        for (int n = k * NT; n < std::min(N, (k + 1) * NT); ++n) {
+            int last_t = -1;
+            for (int e = off[n]; e < off[n + 1]; ++e) {
+                const int t = ent[e] / 6, slot = ent[e] % 6;
+                const int li = (int)(std::lower_bound(L0, L1, t) - L0);
+                if (L0 + li == L1 || L0[li] != t || t < last_t) {
+                    err = "incidence lists disagree with the patches";
+                    return false;
+                }
+                last_t = t;
+                const int c = L.tile_chunk[k] + li / kTile;
+                const int j = n - k * NT;
+                if (run_last[c] != j) {
+                    L.run_node[c].push_back((unsigned short)j);
+                    L.run_end[c].push_back(L.run_end[c].empty() ? 0 : L.run_end[c].back());
+                    run_last[c] = j;
+                }
+                L.cent[c].push_back((unsigned short)(slot * 3 * kTile + li % kTile));
+                L.run_end[c].back() += 1;
+            }
+        }
+    }
+    L.fixed = tile_record_bytes(mixed);
+    L.ns_max = 16;
+    L.bytes.assign(C, 0);
+    for (int k = 0; k < K; ++k) {
+        for (int c = L.tile_chunk[k]; c < L.tile_chunk[k + 1]; ++c) {
+            const long long first = L.start[k] + (long long)(c - L.tile_chunk[k]) * kTile;
+            const int ntri = (int)std::max<long long>(0, std::min<long long>(kTile, L.start[k + 1] - first));
+            const size_t R = L.run_node[c].size(), E = L.cent[c].size();
+            // What the kernel indexes: entries inside the chunk's live slots,
+            // run nodes inside the tile's accumulators, run ends ascending up
+            // to E, everything inside one record.
+            bool ok = R <= 6 * kTile && E <= 6 * kTile;
+            for (size_t r = 0; ok && r < R; ++r)
+                ok = L.run_node[c][r] < NT && L.run_end[c][r] > (r ? L.run_end[c][r - 1] : 0);
+            ok = ok && (R == 0 ? E == 0 : L.run_end[c][R - 1] == E);
+            for (size_t e = 0; ok && e < E; ++e)
+                ok = L.cent[c][e] / (3 * kTile) < 6 && L.cent[c][e] % (3 * kTile) < ntri;
+            if (!ok) {
+                err = "node tile chunk fails its bounds";
+                return false;
+            }
+            const size_t ns = (16 + 4 * R + 2 * E + 15) / 16 * 16;
+            L.ns_max = std::max(L.ns_max, ns);
+            L.bytes[c] = (unsigned)(L.fixed + ns);
+        }
+    }
+    L.stride = L.fixed + (L.ns_max + 127) / 128 * 128;
+    return true;
+}
+
+bool choose_node_tiles(const int* patch_ids, int N, int T, int mixed, int sms, int target, int nt_max, int nt_min,
+                       const std::vector<int>& off, const std::vector<int>& ent,
+                       const std::function<int(size_t)>& blocks_for, NodeTileLayout& L, int& NT, int& blocks,
+                       std::string& err) {
+    blocks = 0;
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        const long long slots = (long long)std::max(sms, 1) * target;
+        const long long k = std::max(1LL, (N + slots * nt_max - 1) / (slots * nt_max));
+        NT = std::max(std::min(nt_max, nt_min), (int)((N + k * slots - 1) / (k * slots)));
+        L = NodeTileLayout();
+        if (!node_tile_layout(patch_ids, N, T, NT, mixed, off, ent, L, err)) return false;
+        const size_t smem = node_tile_smem(L.stride, NT, mixed);
+        blocks = smem > 227 * 1024 ? 0 : blocks_for(smem);
+        if (blocks >= target) break;
+        nt_max = nt_max * 7 / 8;
+    }
+    return true;
+}
+
+void fill_node_tile_records(const NodeTileLayout& L, const int* patch_ids, const double* coef_d, const float* coef_f,
+                            const double* area, const double* aux4, int mixed, std::vector<unsigned char>& buf,
+                            std::vector<int>& chunk_tri) {
+    const size_t stride = L.stride, fixed = L.fixed;
+    buf.assign(stride * L.C, 0);
+    chunk_tri.assign((size_t)L.C * kTile, -1);
+    const size_t ids_b = 6 * kTile * 4, coef_b = 24 * kTile * (mixed ? 4 : 8);
+    for (int k = 0; k < L.K; ++k) {
+        for (int c = L.tile_chunk[k]; c < L.tile_chunk[k + 1]; ++c) {
+            unsigned char* r = buf.data() + stride * c;
+            int32_t* ids = reinterpret_cast<int32_t*>(r);
+            double* aux = reinterpret_cast<double*>(r + ids_b + coef_b);
+            const long long first = L.start[k] + (long long)(c - L.tile_chunk[k]) * kTile;
+            const int ntri = (int)std::max<long long>(0, std::min<long long>(kTile, L.start[k + 1] - first));
+            for (int i = 0; i < ntri; ++i) {
+                const int t = L.lst[first + i];
+                chunk_tri[(size_t)c * kTile + i] = t;
+                for (int q = 0; q < 6; ++q) ids[q * kTile + i] = patch_ids[6LL * t + q];
+                if (mixed) {
+                    float* cf = reinterpret_cast<float*>(r + ids_b);
+                    for (int q = 0; q < 24; ++q)
+                        cf[q * kTile + i] = coef_f ? coef_f[24LL * t + q] : (float)coef_d[24LL * t + q];
+                } else {
+                    double* cf = reinterpret_cast<double*>(r + ids_b);
+                    for (int q = 0; q < 24; ++q) cf[q * kTile + i] = coef_d[24LL * t + q];
+                }
+                if (aux4) {
+                    for (int q = 0; q < 4; ++q) aux[q * kTile + i] = aux4[4LL * t + q];
+                } else {
+                    aux[i] = area[t];
+                    aux[kTile + i] = 1.0;
+                }
+            }
+            int32_t* hd = reinterpret_cast<int32_t*>(r + fixed);
+            const int R = (int)L.run_node[c].size(), E = (int)L.cent[c].size();
+            hd[0] = R;
+            hd[1] = E;
+            hd[2] = ntri;
+            unsigned short* u = reinterpret_cast<unsigned short*>(r + fixed + 16);
+            std::copy(L.run_node[c].begin(), L.run_node[c].end(), u);
+            std::copy(L.run_end[c].begin(), L.run_end[c].end(), u + R);
+            std::copy(L.cent[c].begin(), L.cent[c].end(), u + 2 * R);
+        }
+    }
+}
+
+}  // namespace msb

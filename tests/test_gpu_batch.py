@@ -136,3 +136,27 @@ def test_batch_mixed_precision_shapes(tmp_path):
         out.append([b.download(i)[0] for i in range(2)])
     for i in range(2):
         assert np.abs(out[1][i] - out[0][i]).max() < 1e-5
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_node_tiles_bitwise(tmp_path, precision):
+    """The node-tiled one-kernel schedule gives the bits of the two-kernel
+    tile schedule, through dialling, checks, one instance reaching its final
+    equilibrium and one failing on the guard."""
+    from morphoshell_b200 import MS_INST_DONE, MS_INST_FAILED, Batch
+    models, _ = _members(tmp_path, [12, 13, 14], spacing_range=(0.07, 0.1))
+    bad = models[2].dofs(1).copy()
+    bad[2 * models[2].num_nodes + 5] += 1e6
+    out = []
+    for sched in ((-1, 0), (0, 256)):
+        b = Batch(models, precision=precision, dofs=[None, None, bad])
+        b.set_schedule(sched[0], sched[1], 32)
+        steps = b.run(400_000)
+        sts = [b.status(i) for i in range(3)]
+        out.append((steps, [(s.status, s.stepcount, s.equilibria) for s in sts],
+                    [b.download(i) for i in range(3)]))
+        assert sts[2].status == MS_INST_FAILED
+        assert sts[0].status == MS_INST_DONE and sts[1].status == MS_INST_DONE
+    assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
+    for i in range(3):
+        assert np.array_equal(out[0][2][i][0], out[1][2][i][0]) and np.array_equal(out[0][2][i][1], out[1][2][i][1])
