@@ -1,7 +1,9 @@
 // Batched ensembles (ms_batch_* in include/morphoshell_gpu.h).
 //
 // The instances' tables are concatenated into one union mesh; every step is
-// four kernels over the whole union:
+// k_batch_pre, the force step (k_batch_node_tiles alone, the node-tiled
+// schedule, or k_batch_tri / k_batch_tri_tiles then k_batch_node) and
+// k_batch_post over the whole union:
 //   k_batch_pre   one thread per instance: the top of main.cpp's loop body
 //                 (dial factor clamp :286-288, end of a dial phase :293-304,
 //                 whether this step checks for equilibrium) and the
@@ -746,7 +748,8 @@ ms_status ms_batch_create(const ms_batch_instance* inst, int32_t n, int32_t devi
     p.tri_idx = d_idx;
     p.tri_aux = d_aux;
     p.lce_uniform = 1;
-    // Tile records for the bulk-copy tile kernel (the default schedule).
+    // Tile records for the bulk-copy tile kernel (the default schedule on
+    // unions too small for the node-tiled one).
     {
         const int mixed = precision == MS_PRECISION_MIXED;
         int blocks = 0;

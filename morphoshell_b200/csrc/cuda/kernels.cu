@@ -1,7 +1,9 @@
 // sm_100a kernels of the force-and-dynamics loop.
 //
-// Fused path, two kernels per step: the per-triangle kernel k_tri_aos
-// (cluster.cu) writes each triangle's 6 per-node force contributions, then
+// Two-kernel fused path (ms_set_step_path 1 and 2; the default on meshes too
+// small for the node-tiled one-kernel step of node_tiles.cu): the
+// per-triangle kernel (k_tri_aos in cluster.cu, or k_tri_tiles in
+// tri_tiles.cu) writes each triangle's 6 per-node force contributions, then
 //   k_node_update one thread per node: deterministic gather of its
 //                 contributions in ascending triangle order (the transposed
 //                 SpMV of calc_deformation_forces.cpp:185), damping

@@ -1,6 +1,7 @@
-// Shared pieces of the bulk-copy-fed per-triangle kernels (tri_tiles.cu,
-// batch.cu): the tile record layout, and the 1-D bulk copy into shared
-// memory with its mbarrier (no multicast; every wait bounded).
+// Shared pieces of the bulk-copy-fed kernels (tri_tiles.cu, batch.cu,
+// node_tile_walk.cuh): the tile record layout, the 1-D bulk copy into shared
+// memory with its mbarrier (no multicast; every wait bounded) and the
+// per-triangle arithmetic of a record slot.
 #pragma once
 
 #include <cstdint>
