@@ -232,9 +232,14 @@ def run_reference(args):
 
 
 def workload_config(args, model):
-    return {"workload": "%s: unit disk, jittered hex spacing 0.002, %d nodes, %d triangles, LCE protocol-3 "
-                        "dialling (lambda 1 -> 0.85), bbar = 0, h = 0.01, nu = 0.5" % (
-                            args.workload, model.num_nodes, model.num_tris),
+    if args.workload == "disk1p8m":
+        shape = "jittered hex spacing 0.002, wavy azimuthal director, lambda 1 -> 0.85"
+    elif args.workload == "disk18k":
+        shape = "jittered hex spacing 0.02, azimuthal director, lambda 1 -> 0.9"
+    else:
+        shape = "jittered hex spacing %g, azimuthal director, lambda 1 -> 0.9" % (int(args.workload[4:]) / 1000.0)
+    return {"workload": "%s: unit disk, %s, %d nodes, %d triangles, LCE protocol-3 dialling, bbar = 0, h = 0.01, "
+                        "nu = 0.5" % (args.workload, shape, model.num_nodes, model.num_tris),
             "precision": args.precision, "path": args.path, "num_tris": model.num_tris, "num_nodes": model.num_nodes,
             "l2": "inputs larger than L2 (~1 GB moved per step vs 126 MB L2); no flush",
             "parallelism": "replicas x%d" % args.gpus}
