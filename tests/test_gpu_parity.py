@@ -140,9 +140,11 @@ def test_fused_step_matches_per_function_path(workdir):
     assert rel_err(v1, v2) < 1e-10
 
 
-def test_fused_steps_vs_oracle_1e4(workdir):
+@pytest.mark.parametrize("path", [2, 3])
+def test_fused_steps_vs_oracle_1e4(workdir, path):
     """10^4 fused dialling steps from the flat, noisy initial state against the
-    oracle: node positions within 1e-9 relative."""
+    oracle, on the two-kernel and on the node-tiled step: node positions
+    within 1e-9 relative."""
     from morphoshell_b200 import GpuLoop
     from oracle import Oracle
     m = make_model(workdir, "disk100")
@@ -153,6 +155,7 @@ def test_fused_steps_vs_oracle_1e4(workdir):
     k = np.arange(n)
     dials = s.dial_factors_to_hold_at_spacing * (k / s.timesteps_per_dial_phase)
     g, o = GpuLoop(m), Oracle("orc", m)
+    g.set_step_path(path)
     for t in (g, o):
         t.set_programmed(3, a_info, b_info, s.dial_factors_to_hold_at_spacing)
         t.upload(x0)
