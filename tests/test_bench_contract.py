@@ -46,3 +46,18 @@ def test_reference_arm_json_line():
     assert line["impl"] == "reference" and line["value"] > 0 and line["e2e"]["h2d_bytes_per_step"] == 0
     assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["cores"] >= 1
     assert "spacing 0.05" in line["config"]["workload"]
+
+
+def test_reference_arm_under_torchrun_prints_one_line():
+    """Launched as the multi-GPU bench is (torchrun, two ranks), the reference
+    arm runs on rank 0 alone and prints exactly one JSON line."""
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
+           "127.0.0.1", "--master-port", "29631", "bench.py", "--impl", "reference", "--gpus", "2",
+           "--workload", "disk50", "--steps", "3", "--warmup", "3"]
+    out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600, env=env)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
