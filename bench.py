@@ -10,11 +10,13 @@ with an azimuthal director perturbed by 0.3 sin(3 theta) and lambda dialled
 synthetic inputs (there is no public dataset for this path).  A step is one
 timestep of the dialling phase: surface derivatives, in-line dialling,
 deformation forces, damping, constraints, force guard and symplectic Euler
-update -- the fused GPU stepper launches two kernels per step.  Per-step
-traffic is ~1 GB, far above the 126 MB L2, so no flush is needed between
-steps.
+update -- one kernel per step on the node-tiled paths (the warp-specialised
+one is the default at this size).  Per-step traffic is ~0.7 GB, far above the 126 MB L2, so no flush is
+needed between steps.
 
-``value``: K * T * N / (max over ranks of the device time of K steps).
+``value``: K * T * N / (max over ranks of the device time of K steps), FP64.
+``mixed``: the same K steps on the mixed-precision path (FP32 per-triangle
+arithmetic), with its ratio to FP64 and its force error against FP64.
 ``e2e``: the same metric with the state on the host, through the C ABI, every
 step: pinned host dofs + velocities copied in (ms_upload_dofs), one fused step
 (ms_step_n), dofs + velocities copied back (ms_download_dofs).
@@ -188,8 +190,34 @@ def cpu_baseline(model, info, bbar, budget_s: float = 20.0):
             "kind": "reference" if kind == "ref" else "port",
             "sample": "%d steps of the full %d-triangle mesh (protocol-3 dialling) after 1 warm-up step, %d threads"
                       % (n, model.num_tris, cores),
+            "note": SHIM_NOTE if kind == "ref" else "the oracle port (reference build absent)",
             "single_thread_value": model.num_tris * n1 / el1,
             "single_thread_sample": "%d steps, 1 thread" % n1}
+
+
+# The reference's own code runs against this project's stand-in for Eigen 3
+# (oracle/eigen_shim: Eigen is not installed and cannot be fetched here), so
+# its sparse products and vector temporaries are the stand-in's.
+SHIM_NOTE = ("reference sources compiled unmodified against oracle/eigen_shim, this project's stand-in for the "
+             "Eigen 3 subset they use (Eigen is absent here); its sparse x dense product allocates a fresh result "
+             "vector per call, and real Eigen's threaded product may run faster or slower")
+
+
+def reference_workload(name: str, seed: int = 1):
+    """The workload written to a settings file and a mesh file and set up by
+    the reference's own code (oracle.RefSetup), with the programmed fields;
+    the mesh generator is pure Python, so the process maps no library of
+    this project."""
+    import oracle
+    from morphoshell_b200 import meshgen
+    mesh, info, bbar = meshgen.workload(name, seed=seed)
+    d = tempfile.mkdtemp(prefix="ms_ref_")
+    st = os.path.join(d, "settings.txt")
+    vtk = os.path.join(d, "%s.vtk" % name)
+    meshgen.write_settings(st, protocol=3)
+    meshgen.write_vtk(vtk, "%s seed %d" % (name, seed), mesh.nodes, mesh.tris, info, bbar,
+                      ref_thicknesses=np.full(mesh.num_tris, 0.01))
+    return oracle.RefSetup(st, vtk, mesh.num_nodes, mesh.num_tris), info, bbar
 
 
 def run_reference(args):
@@ -197,17 +225,20 @@ def run_reference(args):
     if rank != 0:
         return 0
     import oracle
-    model, info, bbar = make_workload(args.workload)
     kind = "ref" if oracle.available("ref") else "orc"
+    if kind == "ref":
+        model, info, bbar = reference_workload(args.workload)
+    else:
+        model, info, bbar = make_workload(args.workload)
     cores = os.cpu_count() or 1
     o = oracle.Oracle(kind, model, threads=cores)
     s = model.scalars
     o.set_programmed(3, info, bbar, s.dial_factors_to_hold_at_spacing)
     o.upload(model.dofs(1))
     dials = dial_sequence(model, args.warmup + args.steps + 1)
-    # Warm-up (at most 2 steps: each is a full CPU step of the whole mesh),
-    # then as many of the K steps as fit in ~60 s of host time.
-    w = min(args.warmup, 2)
+    # W warm-up steps (each a full CPU step of the whole mesh), then as many
+    # of the K steps as fit in ~60 s of host time.
+    w = args.warmup
     t0 = time.perf_counter()
     o.step_n(w, dials[:w], s.timestep, s.damping_factor_1)
     one = (time.perf_counter() - t0) / max(w, 1)
@@ -224,7 +255,11 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores,
                          "kind": "reference" if kind == "ref" else "port",
                          "sample": "%d of the requested %d steps of the full mesh, %d threads"
-                                   % (n, args.steps, cores)},
+                                   % (n, args.steps, cores),
+                         "note": SHIM_NOTE if kind == "ref" else "the oracle port (reference build absent)",
+                         "setup": "the reference's own set-up code (read_settings, read_vtk_data, calc_mesh_info, "
+                                  "set_up_patch_fitting, calc_dof_masses, noise)" if kind == "ref" else
+                                  "this project's host set-up"},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -240,14 +275,99 @@ def workload_config(args, model):
         shape = "jittered hex spacing %g, azimuthal director, lambda 1 -> 0.9" % (int(args.workload[4:]) / 1000.0)
     return {"workload": "%s: unit disk, %s, %d nodes, %d triangles, LCE protocol-3 dialling, bbar = 0, h = 0.01, "
                         "nu = 0.5" % (args.workload, shape, model.num_nodes, model.num_tris),
-            "precision": args.precision, "path": args.path, "num_tris": model.num_tris, "num_nodes": model.num_nodes,
-            "l2": "inputs larger than L2 (~1 GB moved per step vs 126 MB L2); no flush",
+            "precision": args.precision, "num_tris": model.num_tris, "num_nodes": model.num_nodes,
+            "l2": ("inputs larger than L2 (%.2f GB of tables and node state per step vs 126 MB L2); no flush"
+                   % (BYTES_PER_TRI["fp64"] * model.num_tris / 1e9)
+                   if BYTES_PER_TRI["fp64"] * model.num_tris > 126e6 else
+                   "working set smaller than L2 (a test-size workload); no flush"),
             "parallelism": "replicas x%d" % args.gpus}
+
+
+KERNEL_NAMES = {"cluster": ("k_cluster_step", "k_halo_update"), "two-kernel": ("k_tri_aos", "k_node_update"),
+                "tiles": ("k_tri_tiles", "k_node_update"), "node-tiles": ("k_node_tiles", None),
+                "node-pipe": ("k_node_pipe", None)}
+PATH_IDS = {"cluster": 0, "two-kernel": 1, "tiles": 2, "node-tiles": 3, "node-pipe": 4}
+
+
+def timed_steps(model, info, bbar, precision, path, args, dials, local, dist, clock=None):
+    """One handle at `precision`: W warm-up steps, then K fused steps timed
+    with CUDA events on the library's stream (barrier + synchronize on both
+    sides, max over ranks), then the per-launch kernel times for the
+    roofline.  Returns (handle, ms of the K steps, kernel ms, path name)."""
+    import contextlib
+
+    import torch
+    from morphoshell_b200 import MS_PRECISION_FP64, MS_PRECISION_MIXED, GpuLoop
+    s = model.scalars
+    prec = MS_PRECISION_MIXED if precision == "mixed" else MS_PRECISION_FP64
+    g = GpuLoop(model, precision=prec, device=local)
+    if path != "auto":
+        g.set_step_path(PATH_IDS[path])
+    path = {v: k for k, v in PATH_IDS.items()}[g.plan_info()["path"]]
+    g.set_programmed(3, info, bbar, s.dial_factors_to_hold_at_spacing)
+    g.upload(model.dofs(1))
+    dt, damp = s.timestep, s.damping_factor_1
+    g.step_n(args.warmup, dials[:args.warmup], dt, damp)
+    stream = torch.cuda.ExternalStream(g.stream(), device=torch.device("cuda", local))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with (clock or contextlib.nullcontext()):
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        g.step_n(args.steps, dials[args.warmup:args.warmup + args.steps], dt, damp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    # Per-kernel device time for the roofline (CUDA events on the library's
+    # stream, from a copy of the state so the run above stays as it ended).
+    x, v = g.download()
+    t_tri, t_node = g.time_kernels(50, dial=float(dials[args.warmup]), dt=dt, damping=damp)
+    g.upload(x, v)
+    tri_name, node_name = KERNEL_NAMES[path]
+    kernel_ms = {tri_name: t_tri} if node_name is None else {tri_name: t_tri, node_name: t_node}
+    return g, ms_max, kernel_ms, path
+
+
+def roofline(model, precision, path, workload, kernel_ms):
+    T = model.num_tris
+    bpt = BYTES_PER_TRI[precision]
+    step_ms = sum(kernel_ms.values())
+    achieved = bpt * T / (step_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": profiled_traffic(workload, precision, path), "peak_kind": peak_kind,
+            "kernel": "one step = " + " + ".join(kernel_ms), "algorithmic_bytes_per_tri": bpt,
+            "kernel_ms": kernel_ms}
+
+
+def launches(path, steps):
+    per_step = 1 if KERNEL_NAMES[path][1] is None else 2
+    return per_step * steps + (steps + 127) // 128  # + one chunk-end kernel per captured graph of 128 steps
+
+
+def force_difference(g_a, g_b, x, v, dial):
+    """max |F_a - F_b| / max |F_b| of the deformation forces of two handles on
+    the same state and dial factor."""
+    out = []
+    for g in (g_a, g_b):
+        g.upload(x, v)
+        g.surface_derivs()
+        g.do_dialling(dial)
+        f, _ = g.deformation_forces()
+        out.append(f)
+    return float(np.abs(out[0] - out[1]).max() / np.abs(out[1]).max())
 
 
 def run_ours(args):
     import torch
-    from morphoshell_b200 import MS_PRECISION_FP64, MS_PRECISION_MIXED, GpuLoop, lib
+    from morphoshell_b200 import lib
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -263,55 +383,21 @@ def run_ours(args):
     model, info, bbar = make_workload(args.workload)
     s = model.scalars
     T = model.num_tris
-    prec = MS_PRECISION_MIXED if args.precision == "mixed" else MS_PRECISION_FP64
-    g = GpuLoop(model, precision=prec, device=local)
-    names = {"cluster": 0, "two-kernel": 1, "tiles": 2, "node-tiles": 3}
-    if args.path != "auto":
-        g.set_step_path(names[args.path])
-    plan = g.plan_info()
-    args.path = {v: k for k, v in names.items()}[plan["path"]]
-    g.set_programmed(3, info, bbar, s.dial_factors_to_hold_at_spacing)
-    g.upload(model.dofs(1))
     dials = dial_sequence(model, args.warmup + args.steps + 64)
     dt, damp = s.timestep, s.damping_factor_1
-
-    g.step_n(args.warmup, dials[:args.warmup], dt, damp)
-    stream = torch.cuda.ExternalStream(g.stream(), device=torch.device("cuda", local))
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        e0.record(stream)
-        g.step_n(args.steps, dials[args.warmup:args.warmup + args.steps], dt, damp)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    clk = ClockSampler(local)
+    g, ms_max, kernel_ms, path = timed_steps(model, info, bbar, args.precision, args.path, args, dials, local, dist,
+                                             clock=clk)
     value = T * args.steps * world / (ms_max / 1e3)
-
-    # Per-kernel device time for the roofline (CUDA events on the library's stream).
-    t_tri, t_node = g.time_kernels(50, dial=float(dials[args.warmup]), dt=dt, damping=damp)
-    step_ms = t_tri + t_node
-    bpt = BYTES_PER_TRI[args.precision]
-    achieved = bpt * T / (step_ms / 1e3) / 1e9
-    peak, peak_kind = measured_peak_hbm()
-    traffic = profiled_traffic(args.workload, args.precision, args.path)
 
     # End to end through the C ABI with the state on the host every step.
     N = model.num_nodes
     hx = torch.empty(3 * N, dtype=torch.float64, pin_memory=True).numpy()
     hv = torch.empty(3 * N, dtype=torch.float64, pin_memory=True).numpy()
-    g.download()
     hx[:], hv[:] = g.download()
     e2e_steps = min(args.steps, 200)
     dl = dials[args.warmup:args.warmup + e2e_steps]
+    stream = torch.cuda.ExternalStream(g.stream(), device=torch.device("cuda", local))
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -330,33 +416,47 @@ def run_ours(args):
         L.ms_download_dofs(g._h, pd(hx), pd(hv))
     e3.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e2.elapsed_time(e3)
-    t2 = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    t2 = torch.tensor([e2.elapsed_time(e3)], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(t2, op=dist.ReduceOp.MAX)
     e2e_value = T * e2e_steps * world / (float(t2.item()) / 1e3)
+    n_launch = launches(path, args.steps)
 
-    clocks = clk.summary()
-    tri_name, node_name = {"cluster": ("k_cluster_step", "k_halo_update"), "two-kernel": ("k_tri_aos", "k_node_update"),
-                           "tiles": ("k_tri_tiles", "k_node_update"), "node-tiles": ("k_node_tiles", None)}[args.path]
-    kernels_per_step = 1 if node_name is None else 2
-    kernel_ms = {tri_name: t_tri} if node_name is None else {tri_name: t_tri, node_name: t_node}
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed", "data": "synthetic",
         "config": workload_config(args, model),
-        "gpu_launches": kernels_per_step * args.steps + (args.steps + 127) // 128,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "one step = " + " + ".join(k for k in (tri_name, node_name) if k),
-                     "algorithmic_bytes_per_tri": bpt,
-                     "kernel_ms": kernel_ms},
-        "plan": plan,
+        "step_path": path,
+        "gpu_launches": n_launch,
+        "roofline": roofline(model, args.precision, path, args.workload, kernel_ms),
+        "plan": g.plan_info(),
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 2 * 24 * N + 8,
                 "d2h_bytes_per_step": 2 * 24 * N + 16, "steps": e2e_steps},
-        "clocks": clocks,
+        "clocks": clk.summary(),
     }
+
+    # The other half of the metric: the mixed-precision path on the same mesh,
+    # steps and dial factors, with its force error against FP64 on the state
+    # the FP64 run ended in.
+    if args.precision == "fp64" and not args.no_mixed:
+        clk_m = ClockSampler(local)
+        gm, ms_m, kernel_m, path_m = timed_steps(model, info, bbar, "mixed", args.path, args, dials, local, dist,
+                                                 clock=clk_m)
+        xm, _ = gm.download()
+        x64, v64 = g.download()
+        dial_last = float(dials[args.warmup + args.steps - 1])
+        ferr = force_difference(gm, g, x64, v64, dial_last)
+        value_m = T * args.steps * world / (ms_m / 1e3)
+        line["mixed"] = {
+            "value": value_m, "unit": METRIC, "ms_per_step": ms_m / args.steps, "ratio_vs_fp64": value_m / value,
+            "step_path": path_m, "roofline": roofline(model, "mixed", path_m, args.workload, kernel_m),
+            "max_force_err_vs_fp64": ferr,
+            "max_position_diff_vs_fp64": float(np.abs(xm - x64).max() / np.abs(x64).max()),
+            "force_err_state": "the FP64 run's final state, dial factor of its last step",
+            "clocks": clk_m.summary()}
+        line["gpu_launches"] = n_launch + launches(path_m, args.steps)
+        gm.close()
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(model, info, bbar)
     g.close()
@@ -516,7 +616,9 @@ def main():
     ap.add_argument("--workload", default="disk1p8m")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
-    ap.add_argument("--path", choices=["auto", "cluster", "two-kernel", "tiles", "node-tiles"], default="auto",
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision half of the line")
+    ap.add_argument("--path", choices=["auto", "cluster", "two-kernel", "tiles", "node-tiles", "node-pipe"],
+                    default="auto",
                     help="fused-step implementation (ms_set_step_path); auto: the library's default")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -148,11 +148,11 @@ ms_status ms_advance_dynamics(ms_handle* h, double timestep, double damping_fact
                               int64_t* offending_dof, double* offending_force);
 
 /* Deformation forces (forces = -D^T dE/dcq, as ms_deformation_forces) for
- * callers that cannot allocate device memory: code running while a CUDA
- * graph is captured around it, host frameworks that route every device
- * allocation through their own pool, real-time loops that must not allocate
- * after start-up.  No counterpart in the reference (which never touches a
- * GPU).  No handle is needed and nothing is allocated: every pointer is a
+ * callers that cannot allocate device memory: host frameworks that route
+ * every device allocation through their own pool (an allocation behind the
+ * pool's back breaks its accounting), real-time loops that must not allocate
+ * after start-up (cudaMalloc can block for an unbounded time).  No
+ * counterpart in the reference (which never touches a GPU).  No handle is needed and nothing is allocated: every pointer is a
  * DEVICE pointer the caller owns -- patch_ids 6T, deriv_coeffs 24T, ref_area,
  * ref_thickness, ref_shear_modulus T, abar and bbar 3T (all in the
  * ms_mesh_desc / row-major layouts above), dofs and forces 3N SoA.  Work
@@ -164,7 +164,10 @@ ms_status ms_advance_dynamics(ms_handle* h, double timestep, double damping_fact
  * that first call before any stream capture.  All calls share the array:
  * calls that overlap on the GPU race, so serialise them.  Runs on `stream`
  * (a cudaStream_t, NULL for the default stream) and returns after the forces
- * are written.  err (err_len bytes, may be NULL) receives a message. */
+ * are written (it waits for the stream, to check the patch ids).  A CUDA
+ * error already pending when it is called is reported as MS_ERR_CUDA and
+ * left pending; nothing is launched then.  err (err_len bytes, may be NULL)
+ * receives a message. */
 ms_status ms_deformation_forces_noalloc(int32_t num_nodes, int32_t num_tris, const int32_t* patch_ids,
                                         const double* deriv_coeffs, const double* ref_area,
                                         const double* ref_thickness, const double* ref_shear_modulus,
@@ -175,8 +178,12 @@ ms_status ms_deformation_forces_noalloc(int32_t num_nodes, int32_t num_tris, con
 /* ---- fused stepper: the whole main.cpp:308-488 body per step ----------
  * Runs n steps of: surface derivs -> (dialling) -> deformation forces ->
  * damping -> constraints -> (equilibrium check on the last step if
- * check_last) -> force guard -> symplectic Euler, as two kernels per step
- * captured in a CUDA graph.  dial_factors[i] (length n, may be NULL when
+ * check_last) -> force guard -> symplectic Euler, as one kernel per step on
+ * the node-tiled path (two on the others, ms_set_step_path) captured in CUDA
+ * graphs.  Fused protocol-3 steps dial inside the force kernel; the abar and
+ * bbar arrays are brought to the last step's dial factor only when a later
+ * call reads them (ms_download_programmed, ms_deformation_forces,
+ * ms_output_quantities, non-fused steps).  dial_factors[i] (length n, may be NULL when
  * dialling == 0) is the dial factor step i dials to.  Stops at the first
  * step whose force guard trips and reports it; the state is then the state
  * before that step, as in main.cpp:448-474. */

@@ -441,8 +441,10 @@ class GpuLoop:
     def set_step_path(self, path: int):
         """0: cluster-tiled step, 1: two-kernel step, 2: two-kernel step with
         the per-triangle tables fed by bulk asynchronous copies, 3: node-tiled
-        one-kernel step (forces summed in shared memory per tile of nodes;
-        the default on meshes with a node tile for every resident block)."""
+        one-kernel step (forces summed in shared memory per tile of nodes),
+        4: the node-tiled step with warp-specialised roles (two warpgroups
+        compute triangles while a third sums and updates nodes; the default
+        on meshes with a node tile for every SM)."""
         self._chk(lib().ms_set_step_path(self._h, path), "set_step_path")
 
     def plan_info(self) -> dict:

@@ -34,7 +34,8 @@ NVCCFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xco
 
 HOST_SOURCES = ["host/settings.cpp", "host/vtk_io.cpp", "host/mesh_setup.cpp", "host/host_capi.cpp"]
 CUDA_SOURCES = ["cuda/kernels.cu", "cuda/cluster.cu", "cuda/capi.cu", "cuda/noalloc.cu", "cuda/batch.cu",
-                "cuda/learned.cu", "cuda/tri_tiles.cu", "cuda/node_tiles.cu", "cuda/node_tile_plan.cu"]
+                "cuda/learned.cu", "cuda/tri_tiles.cu", "cuda/node_tiles.cu", "cuda/node_tile_plan.cu",
+                "cuda/node_pipe.cu"]
 HEADERS = ["host/host.hpp", "host/small_linalg.hpp", "cuda/internal.cuh", "cuda/tri_physics.cuh", "cuda/step_common.cuh",
            "cuda/tri_contrib.cuh", "cuda/tc_gemm.cuh", "cuda/tile_copy.cuh", "cuda/node_tile_walk.cuh",
            "../../include/morphoshell_gpu.h", "../../include/morphoshell_host.h"]

@@ -3,6 +3,7 @@
 // stepper captured in CUDA graphs, and the output diagnostics.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -50,6 +51,12 @@ struct ms_handle {
     double spacing = 1.0;
     int from_ansatz = 0;
     bool programmed = false;
+    // The fused protocol-3 steps dial inside the force kernel and never write
+    // abar/bbar.  After them the arrays are stale: they are brought to the
+    // last step's dial factor (stale_dial) by the dialling kernel only when a
+    // call reads them (materialise_programmed), not after every ms_step_n.
+    bool ab_stale = false;
+    double stale_dial = 0.0;
     // allocations
     std::vector<void*> allocs;
     double* d_dials = nullptr;
@@ -71,7 +78,8 @@ struct ms_handle {
     ClusterPlan plan{};
     bool have_plan = false;
     bool have_cluster = false;
-    int step_path = 1;  // 0 cluster-tiled, 1 two-kernel, 2 two-kernel with bulk-copied tiles, 3 node-tiled
+    int step_path = 1;  // 0 cluster-tiled, 1 two-kernel, 2 two-kernel with bulk-copied tiles, 3 node-tiled,
+                        // 4 node-tiled with warp-specialised roles
     std::vector<double> area_host;
     double lce_lam_final = 0, lce_nu = 0;
     int halo_parts = 0;
@@ -81,6 +89,7 @@ struct ms_handle {
     size_t tile_bytes = 0;
     // node-tiled step
     bool have_ntiles = false;
+    bool have_pipe = false;  // warp-specialised node-tiled step
     NodeTilePlan ntp{};
     unsigned char* d_nt_rec = nullptr;
     std::vector<int> nt_chunk_tri;  // host copy of NodeTilePlan::chunk_tri
@@ -169,6 +178,21 @@ ms_status ensure_out(ms_handle* h, size_t bytes) {
 
 bool lce_fusable(const ms_handle* h) { return h->protocol == 3 && !h->from_ansatz && h->precision >= 0; }
 
+// Paths 3 and 4 run the whole step in one kernel.
+bool one_kernel_step(const ms_handle* h) {
+    return (h->step_path == 3 && h->have_ntiles) || (h->step_path == 4 && h->have_pipe);
+}
+
+// Brings abar/bbar up to the dial factor of the last fused step, as
+// do_dialling (do_dialling.cpp:112-123) would have left them, before a call
+// that reads them.  Enqueued on the handle's stream; no synchronisation.
+ms_status materialise_programmed(ms_handle* h) {
+    if (!h->ab_stale) return MS_OK;
+    MS_CUDA(h, launch_dialling(h->m, h->protocol, h->stale_dial, h->spacing, h->from_ansatz, h->stream));
+    h->ab_stale = false;
+    return MS_OK;
+}
+
 template <typename T>
 ms_status upload(ms_handle* h, T** dst, const std::vector<T>& src) {
     MS_TRY(dalloc(h, dst, src.size()));
@@ -237,6 +261,13 @@ ms_status build_tiles(ms_handle* h, const ms_mesh_desc* d) {
 #define MSB_NT_NODES_MIXED 1008
 #endif
 constexpr int kNtNodesMin = 256;
+// Largest nodes per tile of the warp-specialised step (one block per SM): its
+// shared memory holds two table buffers, two staging areas and eight node
+// sections besides the accumulators, and tiles this size leave about 14 % of
+// the triangles on tile borders.
+#ifndef MSB_PIPE_NODES
+#define MSB_PIPE_NODES 1600
+#endif
 
 // Plan of the node-tiled step: the chunk records, area in the trigonometry
 // block (cos^2 = 1, the rest 0) until prepare_lce_tables writes the
@@ -255,8 +286,10 @@ ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vecto
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     NodeTileLayout L;
     std::string err;
-    int NT = 0, blocks = 0;
-    auto blocks_for = [&](size_t smem) {
+    int NT = 0, blocks = 0, pipe_blocks = 0;
+    auto tile_smem = [&](size_t stride, int nodes) { return node_tile_smem(stride, nodes, mixed); };
+    auto pipe_smem = [&](size_t stride, int nodes) { return node_pipe_smem(stride, nodes, mixed); };
+    auto tile_blocks = [&](size_t smem) {
         int b = 0;
         if (prepare_node_tile_kernels(mixed, smem, &b) != cudaSuccess) {
             cudaGetLastError();
@@ -264,11 +297,37 @@ ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vecto
         }
         return b;
     };
-    if (!choose_node_tiles(d->patch_ids, N, T, mixed, sms, node_tile_blocks_target(mixed),
-                           mixed ? MSB_NT_NODES_MIXED : MSB_NT_NODES, kNtNodesMin, off, ent, blocks_for, L, NT, blocks,
-                           err))
-        return fail(h, MS_ERR_INVALID_ARGUMENT, err);
-    if (blocks <= 0) {
+    auto pipe_blocks_for = [&](size_t smem) {
+        int b = 0;
+        if (prepare_node_pipe_kernels(mixed, smem, &b) != cudaSuccess) {
+            cudaGetLastError();
+            b = 0;
+        }
+        return b;
+    };
+    // One plan serves both node-tiled kernels.  Its tiles are sized for the
+    // warp-specialised kernel (path 4, one block per SM) when that kernel
+    // can run, else for the node-tiled kernel (path 3).  MSB_NODE_TILE_PLAN=3
+    // in the environment sizes them for path 3 regardless.
+    const char* plan_env = std::getenv("MSB_NODE_TILE_PLAN");
+    const bool plan3 = plan_env && std::string(plan_env) == "3";
+    if (!plan3) {
+        if (!choose_node_tiles(d->patch_ids, N, T, mixed, sms, 1, MSB_PIPE_NODES, kNtNodesMin, off, ent, pipe_smem,
+                               pipe_blocks_for, L, NT, pipe_blocks, err))
+            return fail(h, MS_ERR_INVALID_ARGUMENT, err);
+        if (pipe_blocks > 0) {
+            blocks = tile_blocks(tile_smem(L.stride, NT));
+        }
+    }
+    if (pipe_blocks <= 0) {
+        if (!choose_node_tiles(d->patch_ids, N, T, mixed, sms, node_tile_blocks_target(mixed),
+                               mixed ? MSB_NT_NODES_MIXED : MSB_NT_NODES, kNtNodesMin, off, ent, tile_smem, tile_blocks,
+                               L, NT, blocks, err))
+            return fail(h, MS_ERR_INVALID_ARGUMENT, err);
+        // The warp-specialised kernel on this plan, where it fits.
+        pipe_blocks = pipe_blocks_for(pipe_smem(L.stride, NT));
+    }
+    if (blocks <= 0 && pipe_blocks <= 0) {
         h->have_ntiles = false;
         return MS_OK;  // the other paths remain
     }
@@ -289,6 +348,7 @@ ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vecto
     q.ntiles = K;
     q.nchunks = C;
     q.grid = sms * blocks;
+    q.grid_pipe = sms * std::min(pipe_blocks, 1);
     q.stride = stride;
     q.rec = d_rec;
     q.tile_chunk = d_tile_chunk;
@@ -296,17 +356,19 @@ ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vecto
     q.chunk_tri = d_ctri;
     h->d_nt_rec = d_rec;
     // One equilibrium partial per block.
-    const int parts = std::min(K, q.grid);
+    const int parts = std::min(K, std::max(q.grid, q.grid_pipe));
     if (parts > h->s.eq_blocks) {
         EqPartial* ep;
         MS_TRY(dalloc(h, &ep, parts));
         h->s.eq_part = ep;
         h->s.eq_blocks = parts;
     }
-    h->have_ntiles = true;
-    // Measured fastest on B200 once every block has a tile of its own
-    // (same bits as paths 1 and 2).
-    if (K >= q.grid) h->step_path = 3;
+    h->have_ntiles = q.grid > 0;
+    h->have_pipe = q.grid_pipe > 0;
+    // The node-tiled kernels once every block has a tile of its own (same
+    // bits as paths 1 and 2): the warp-specialised one where it runs.
+    if (h->have_pipe && K >= q.grid_pipe) h->step_path = 4;
+    else if (h->have_ntiles && K >= q.grid) h->step_path = 3;
     return MS_OK;
 }
 
@@ -713,6 +775,7 @@ ms_status ms_set_programmed(ms_handle* h, int protocol, const double* abar_info,
     if (ka < need_a[protocol] || kb < need_b[protocol])
         return fail(h, MS_ERR_INVALID_ARGUMENT, "abar_info/bbar_info have too few columns for this protocol");
     if (protocol == 4 && !(spacing > 0)) return fail(h, MS_ERR_INVALID_ARGUMENT, "protocol 4 needs spacing > 0");
+    MS_TRY(materialise_programmed(h));
     const size_t T = h->m.T;
     if (h->m.info_a) {
         cudaFree((void*)h->m.info_a);
@@ -742,6 +805,7 @@ ms_status ms_set_programmed(ms_handle* h, int protocol, const double* abar_info,
 
 ms_status ms_set_zero_dial_state(ms_handle* h, const double* a0, const double* b0) {
     if (!h) return MS_ERR_INVALID_ARGUMENT;
+    MS_TRY(materialise_programmed(h));
     const size_t T = h->m.T;
     std::vector<double> ident(3 * T, 0.0);
     for (size_t t = 0; t < T; ++t) {
@@ -759,12 +823,14 @@ ms_status ms_do_dialling(ms_handle* h, double dial) {
     if (!h) return MS_ERR_INVALID_ARGUMENT;
     if (!h->programmed) return fail(h, MS_ERR_INVALID_ARGUMENT, "ms_set_programmed has not been called");
     MS_CUDA(h, launch_dialling(h->m, h->protocol, dial, h->spacing, h->from_ansatz, h->stream));
+    h->ab_stale = false;
     MS_CUDA(h, cudaStreamSynchronize(h->stream));
     return MS_OK;
 }
 
 ms_status ms_download_programmed(ms_handle* h, double* abar, double* bbar) {
     if (!h) return MS_ERR_INVALID_ARGUMENT;
+    MS_TRY(materialise_programmed(h));
     if (abar) MS_TRY(download_transposed<double>(h, abar, h->m.abar, h->m.T, 3));
     if (bbar) MS_TRY(download_transposed<double>(h, bbar, h->m.bbar, h->m.T, 3));
     return MS_OK;
@@ -794,6 +860,7 @@ ms_status ms_a_b_normals(ms_handle* h, double* a, double* b, double* n) {
 
 ms_status ms_deformation_forces(ms_handle* h, double* forces, double* dE) {
     if (!h) return MS_ERR_INVALID_ARGUMENT;
+    MS_TRY(materialise_programmed(h));
     MS_CUDA(h, launch_forces_from_cq(h->m, h->s, dE ? 1 : 0, h->stream));
     MS_CUDA(h, launch_gather_forces(h->m, h->s, h->stream));
     if (forces)
@@ -896,6 +963,8 @@ static cudaError_t launch_step(ms_handle* h, const StepScalars& sc, bool cluster
     if (cluster) {
         e = launch_cluster_step(h->m, h->plan, h->s, sc, dial_mode, h->precision, st);
         if (e == cudaSuccess) e = launch_halo_update(h->m, h->plan, h->s, sc, h->precision, st);
+    } else if (h->step_path == 4 && h->have_pipe) {
+        e = launch_node_pipe(h->m, h->plan, h->ntp, h->s, sc, dial_mode, h->precision, st);
     } else if (h->step_path == 3 && h->have_ntiles) {
         e = launch_node_tiles(h->m, h->plan, h->ntp, h->s, sc, dial_mode, h->precision, st);
     } else {
@@ -909,10 +978,11 @@ static cudaError_t launch_step(ms_handle* h, const StepScalars& sc, bool cluster
 }
 
 ms_status ms_set_step_path(ms_handle* h, int path) {
-    if (!h || path < 0 || path > 3) return MS_ERR_INVALID_ARGUMENT;
+    if (!h || path < 0 || path > 4) return MS_ERR_INVALID_ARGUMENT;
     if (path == 0 && !h->have_cluster) return fail(h, MS_ERR_UNSUPPORTED, "cluster launches are unavailable");
     if (path == 2 && !h->have_tiles) return fail(h, MS_ERR_UNSUPPORTED, "bulk-copy tile kernel unavailable");
     if (path == 3 && !h->have_ntiles) return fail(h, MS_ERR_UNSUPPORTED, "node-tiled kernel unavailable");
+    if (path == 4 && !h->have_pipe) return fail(h, MS_ERR_UNSUPPORTED, "warp-specialised node-tiled kernel unavailable");
     h->step_path = path;
     return MS_OK;
 }
@@ -932,6 +1002,9 @@ ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, doub
     const int dial_mode = fuse_lce ? DIAL_LCE : DIAL_ARRAYS;
     const bool cluster = use_cluster(h, dialling != 0);
     cudaStream_t st = h->stream;
+    // Steps that read abar/bbar from the arrays need them current; fused
+    // protocol-3 steps dial in the kernel and leave them stale.
+    if (!fuse_lce) MS_TRY(materialise_programmed(h));
     if (dialling) MS_TRY(stage_dials(h, dials, n));
     MS_TRY(reset_error(h));
     const int p0 = h->cur;
@@ -939,7 +1012,7 @@ ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, doub
     while (done < n) {
         const int len = std::min(kChunk, n - done);
         const bool last_chunk = done + len == n;
-        GraphKey key{len, p0 ^ (done & 1), dial_mode + (cluster ? 16 : 0) + (h->step_path == 2 ? 32 : 0) + (h->step_path == 3 ? 64 : 0), gd,
+        GraphKey key{len, p0 ^ (done & 1), dial_mode + (cluster ? 16 : 0) + 32 * h->step_path, gd,
                      (check_last && last_chunk) ? 1 : 0,
                      dt, damping};
         cudaGraphExec_t exec = nullptr;
@@ -1000,7 +1073,10 @@ ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, doub
         h->cur = p0 ^ (step & 1);
         // Recompute the failing step's forces from its saved input state, as
         // the reference holds them when it throws (main.cpp:448-474).
-        if (dialling) MS_CUDA(h, launch_dialling(h->m, h->protocol, dials[step], h->spacing, h->from_ansatz, st));
+        if (dialling) {
+            MS_CUDA(h, launch_dialling(h->m, h->protocol, dials[step], h->spacing, h->from_ansatz, st));
+            h->ab_stale = false;
+        }
         MS_CUDA(h, launch_surface_derivs(h->m, h->s, h->cur, st));
         MS_CUDA(h, launch_forces_from_cq(h->m, h->s, 0, st));
         MS_CUDA(h, launch_gather_forces(h->m, h->s, st));
@@ -1017,11 +1093,11 @@ ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, doub
         }
         return fail(h, MS_ERR_IMPLAUSIBLE_FORCE, "implausibly_high_force");
     }
-    // The fused LCE path never wrote abar/bbar; leave the tensors of the last
-    // dialled step in force, as do_dialling would have.
+    // The fused LCE path never wrote abar/bbar: they stand for the last
+    // dialled step from here on and are formed when a call reads them.
     if (fuse_lce) {
-        MS_CUDA(h, launch_dialling(h->m, h->protocol, dials[n - 1], h->spacing, h->from_ansatz, st));
-        MS_CUDA(h, cudaStreamSynchronize(st));
+        h->ab_stale = true;
+        h->stale_dial = dials[n - 1];
     }
     h->cur = p0 ^ (n & 1);
     if (rep) {
@@ -1041,6 +1117,7 @@ ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial, dou
     if (dialling && !fuse_lce) return fail(h, MS_ERR_UNSUPPORTED, "kernel timing covers the fused protocol-3 path");
     const bool cluster = use_cluster(h, dialling != 0);
     cudaStream_t st = h->stream;
+    if (!fuse_lce) MS_TRY(materialise_programmed(h));
     if (dialling) {
         std::vector<double> d(reps, dial);
         MS_TRY(stage_dials(h, d.data(), reps));
@@ -1054,6 +1131,8 @@ ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial, dou
         const int mode = fuse_lce ? DIAL_LCE : DIAL_ARRAYS;
         MS_CUDA(h, cudaEventRecord(ev[3 * i], st));
         if (cluster) MS_CUDA(h, launch_cluster_step(h->m, h->plan, h->s, sc, mode, h->precision, st));
+        else if (h->step_path == 4 && h->have_pipe)
+            MS_CUDA(h, launch_node_pipe(h->m, h->plan, h->ntp, h->s, sc, mode, h->precision, st));
         else if (h->step_path == 3 && h->have_ntiles)
             MS_CUDA(h, launch_node_tiles(h->m, h->plan, h->ntp, h->s, sc, mode, h->precision, st));
         else if (h->step_path == 2 && h->have_tiles)
@@ -1061,7 +1140,7 @@ ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial, dou
         else MS_CUDA(h, launch_tri_aos(h->m, h->plan, h->s, sc, mode, h->precision, st));
         MS_CUDA(h, cudaEventRecord(ev[3 * i + 1], st));
         if (cluster) MS_CUDA(h, launch_halo_update(h->m, h->plan, h->s, sc, h->precision, st));
-        else if (!(h->step_path == 3 && h->have_ntiles)) MS_CUDA(h, launch_node_update(h->m, h->s, sc, h->precision, st));
+        else if (!one_kernel_step(h)) MS_CUDA(h, launch_node_update(h->m, h->s, sc, h->precision, st));
         MS_CUDA(h, cudaEventRecord(ev[3 * i + 2], st));
         p ^= 1;
     }
@@ -1079,7 +1158,7 @@ ms_status ms_time_kernels(ms_handle* h, int reps, int dialling, double dial, dou
     if (h->h_err->flag) return fail(h, MS_ERR_IMPLAUSIBLE_FORCE, "implausibly_high_force during kernel timing");
     h->cur = p;
     *ms_tri = a / reps;
-    *ms_node = (!cluster && h->step_path == 3 && h->have_ntiles) ? 0.0 : b / reps;  // path 3 has no node kernel
+    *ms_node = (!cluster && one_kernel_step(h)) ? 0.0 : b / reps;  // paths 3 and 4 have no node kernel
     return MS_OK;
 }
 
@@ -1096,11 +1175,12 @@ ms_status ms_plan_info(ms_handle* h, int* cluster_size, int* tris_per_cta, int* 
 
 ms_status ms_node_tile_plan(ms_handle* h, int* nodes_per_tile, int* tiles, int* chunks, int* blocks) {
     if (!h) return MS_ERR_INVALID_ARGUMENT;
-    const bool ok = h->have_ntiles;
+    const bool ok = h->have_ntiles || h->have_pipe;
+    const int grid = h->step_path == 4 ? h->ntp.grid_pipe : h->ntp.grid;
     if (nodes_per_tile) *nodes_per_tile = ok ? h->ntp.nodes : 0;
     if (tiles) *tiles = ok ? h->ntp.ntiles : 0;
     if (chunks) *chunks = ok ? h->ntp.nchunks : 0;
-    if (blocks) *blocks = ok ? std::min(h->ntp.ntiles, h->ntp.grid) : 0;
+    if (blocks) *blocks = ok ? std::min(h->ntp.ntiles, grid) : 0;
     return MS_OK;
 }
 
@@ -1137,6 +1217,7 @@ ms_status ms_output_quantities(ms_handle* h, double* curv, double* edens, double
     if (!h) return MS_ERR_INVALID_ARGUMENT;
     const size_t T = h->m.T, N = h->m.N;
     cudaStream_t st = h->stream;
+    MS_TRY(materialise_programmed(h));
     MS_CUDA(h, launch_surface_derivs(h->m, h->s, h->cur, st));
     MS_TRY(ensure_out(h, (2 * T + 2 * T + T + 8 * T + N) * sizeof(double)));
     double* dcurv = h->d_out;

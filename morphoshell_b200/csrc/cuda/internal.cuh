@@ -127,6 +127,10 @@ struct ClusterPlan {
 
 // Triangles per tile of the bulk-copy-fed per-triangle kernel.
 constexpr int kTile = 128;
+// Node-tiled step: the flag of a node's last run in its tile, and the
+// largest tile the 15 remaining bits of a run's node index can address.
+constexpr unsigned short kRunFinal = 0x8000;
+constexpr int kNtMaxNodes = 32768;
 
 // Node-tiled step (node_tiles.cu): one kernel per step.  The nodes, in their
 // Morton order, are cut into node tiles of `nodes` consecutive nodes.  The
@@ -138,7 +142,9 @@ constexpr int kTile = 128;
 // [24][kTile], area and director trigonometry [4][kTile]) followed by the
 // chunk's node section:
 //   int32 header {R, E, ntri, 0}
-//   uint16 run_node[R]   node (index in the tile) of each run
+//   uint16 run_node[R]   node (index in the tile) of each run; kRunFinal
+//                        set on the node's last run in its tile (an empty
+//                        one for a node with no triangles)
 //   uint16 run_end[R]    end of the run's entries (exclusive, cumulative)
 //   uint16 ent[E]        patch slot * 3 kTile + slot in chunk, per node ascending t
 //                        (the x component of the contribution in the block's
@@ -149,7 +155,8 @@ struct NodeTilePlan {
     int nodes;                       // nodes per tile
     int ntiles;
     int nchunks;
-    int grid;                        // persistent blocks
+    int grid;                        // persistent blocks of the node-tiled kernel (path 3)
+    int grid_pipe;                   // persistent blocks of the warp-specialised kernel (path 4)
     size_t stride;                   // bytes between chunk records
     const unsigned char* rec;        // [nchunks] records (double weights, or float for mixed)
     const int* tile_chunk;           // [ntiles + 1] first chunk of each tile
@@ -181,8 +188,11 @@ bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, con
 // sets up the kernel and returns its resident blocks per SM (0 when it
 // cannot run).  On return `blocks` is the resident blocks of the chosen plan
 // (0: the kernel cannot run); false with err for inconsistent lists.
+// smem_for(stride, nodes) is the kernel's shared memory per block for a
+// layout.
 bool choose_node_tiles(const int* patch_ids, int N, int T, int mixed, int sms, int target, int nt_max, int nt_min,
                        const std::vector<int>& off, const std::vector<int>& ent,
+                       const std::function<size_t(size_t, int)>& smem_for,
                        const std::function<int(size_t)>& blocks_for, NodeTileLayout& L, int& NT, int& blocks,
                        std::string& err);
 // The chunk records of a layout (ids from patch_ids [T][6]; weights from
@@ -318,6 +328,12 @@ cudaError_t launch_tri_tiles(const DevMesh& m, const ClusterPlan& p, const DevSt
 // Node-tiled step (node_tiles.cu): shared memory per block for a plan,
 // kernel set-up (dynamic shared memory; resident blocks per SM) and launch.
 size_t node_tile_smem(size_t stride, int nodes, int mixed);
+// Warp-specialised node-tiled step (node_pipe.cu): shared memory per block,
+// kernel set-up (resident blocks per SM), launch.
+size_t node_pipe_smem(size_t stride, int nodes, int mixed);
+cudaError_t prepare_node_pipe_kernels(int mixed, size_t smem, int* blocks_per_sm);
+cudaError_t launch_node_pipe(const DevMesh& m, const ClusterPlan& p, const NodeTilePlan& q, const DevState& s,
+                             const StepScalars& sc, int dial_mode, int mixed, cudaStream_t st);
 int node_tile_blocks_target(int mixed);
 cudaError_t prepare_node_tile_kernels(int mixed, size_t smem, int* blocks_per_sm);
 cudaError_t launch_node_tiles(const DevMesh& m, const ClusterPlan& p, const NodeTilePlan& q, const DevState& s,

@@ -1,13 +1,15 @@
 // Deformation forces without any device allocation (ms_deformation_forces_noalloc
 // in include/morphoshell_gpu.h).
 //
-// Who needs it: callers that cannot call cudaMalloc -- code that runs while a
-// CUDA graph is being captured around it, host frameworks that own every
-// device allocation through their own pool and forbid others, and real-time
-// loops that must not allocate after start-up.  They already hold device
-// buffers for the mesh tables, the positions and the forces; this entry
-// point computes forces = -D^T dE/dcq from them using a fixed scratch area
-// that lives in this library's static device memory.
+// Who needs it: callers that cannot call cudaMalloc -- host frameworks that
+// route every device allocation through their own pool and forbid others
+// (an allocation behind the pool's back breaks its accounting and can fail
+// once the pool holds the memory), and real-time loops that must not
+// allocate after start-up (cudaMalloc can block on the device and take
+// unbounded time).  They already hold device buffers for the mesh tables, the
+// positions and the forces; this entry point computes forces = -D^T dE/dcq
+// from them using a fixed scratch area that lives in this library's static
+// device memory.
 //
 // Scratch: one file-scope __device__ array sized for meshes of up to
 // kMaxTris triangles and kMaxNodes nodes (about 11.5 MB, held by every GPU
@@ -251,22 +253,45 @@ extern "C" ms_status ms_deformation_forces_noalloc(int32_t num_nodes, int32_t nu
         set_msg(err, err_len, cudaGetErrorString(e));
         return e == cudaErrorNoDevice ? MS_ERR_NO_DEVICE : MS_ERR_CUDA;
     }
+    // An error left pending by the caller's earlier work is not this call's:
+    // report it without clearing it, and launch nothing.
+    e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        char buf[200];
+        std::snprintf(buf, sizeof buf, "ms_deformation_forces_noalloc: a CUDA error was pending before the call (%s)",
+                      cudaGetErrorString(e));
+        set_msg(err, err_len, buf);
+        return MS_ERR_CUDA;
+    }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int N = num_nodes, T = num_tris;
+    // Each launch is checked on its own so the message names the kernel that
+    // failed; the error is ours, so it is cleared.
+    auto launched = [&](const char* name) -> bool {
+        const cudaError_t le = cudaGetLastError();
+        if (le == cudaSuccess) return true;
+        char buf[200];
+        std::snprintf(buf, sizeof buf, "ms_deformation_forces_noalloc: launch of %s failed (%s)", name,
+                      cudaGetErrorString(le));
+        set_msg(err, err_len, buf);
+        return false;
+    };
     k_na_zero<<<(N + 256) / 256, 256, 0, st>>>(s, N);
+    if (!launched("k_na_zero")) return MS_ERR_CUDA;
     k_na_count<<<(6 * T + 255) / 256, 256, 0, st>>>(s, patch_ids, T, N);
+    if (!launched("k_na_count")) return MS_ERR_CUDA;
     k_na_scan<<<1, 1024, 0, st>>>(s, N);
+    if (!launched("k_na_scan")) return MS_ERR_CUDA;
     k_na_fill<<<(6 * T + 255) / 256, 256, 0, st>>>(s, patch_ids, T, N);
+    if (!launched("k_na_fill")) return MS_ERR_CUDA;
     k_na_sort<<<(N + 255) / 256, 256, 0, st>>>(s, N);
+    if (!launched("k_na_sort")) return MS_ERR_CUDA;
     k_na_tri<<<(T + 127) / 128, 128, 0, st>>>(s, N, T, patch_ids, deriv_coeffs, ref_area, ref_thickness,
                                                ref_shear_modulus, abar, bbar, def_poisson_ratio,
                                                bend_stiffening_scale_factor, dofs);
+    if (!launched("k_na_tri")) return MS_ERR_CUDA;
     k_na_gather<<<(N + 255) / 256, 256, 0, st>>>(s, N, forces);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) {
-        set_msg(err, err_len, cudaGetErrorString(e));
-        return MS_ERR_CUDA;
-    }
+    if (!launched("k_na_gather")) return MS_ERR_CUDA;
     // Wait for the result and check the ids (a plain host int: no allocation).
     int bad = 0;
     e = cudaMemcpyAsync(&bad, &s->bad, sizeof(int), cudaMemcpyDeviceToHost, st);

@@ -12,8 +12,8 @@ namespace msb {
 
 bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, const std::vector<int>& off,
                       const std::vector<int>& ent, NodeTileLayout& L, std::string& err) {
-    if (NT <= 0 || NT > 65536) {
-        err = "nodes per tile must be in 1..65536";
+    if (NT <= 0 || NT > kNtMaxNodes) {
+        err = "nodes per tile must be in 1..32768";
         return false;
     }
     const int K = (N + NT - 1) / NT;
@@ -54,6 +54,9 @@ bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, con
     // Node sections: for each chunk, runs (node in tile, end) and entries
     // (patch slot * 3 kTile + slot in chunk).  Nodes go in ascending order and each node's
     // entries in ascending t, so a node's entries within a chunk are one run.
+    // A node's last run in its tile carries kRunFinal: once it is added the
+    // node's force is complete.  A node with no entries gets an empty final
+    // run in its tile's last chunk, so every node of a tile has exactly one.
     L.run_node.assign(C, {});
     L.run_end.assign(C, {});
     L.cent.assign(C, {});
@@ -62,7 +65,14 @@ bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, con
         const int* L0 = L.lst.data() + L.start[k];
         const int* L1 = L.lst.data() + L.start[k + 1];
         for (int n = k * NT; n < std::min(N, (k + 1) * NT); ++n) {
-            int last_t = -1;
+            int last_t = -1, last_c = -1;
+            if (off[n] == off[n + 1]) {
+                const int c = L.tile_chunk[k + 1] - 1;
+                L.run_node[c].push_back((unsigned short)((n - k * NT) | kRunFinal));
+                L.run_end[c].push_back(L.run_end[c].empty() ? 0 : L.run_end[c].back());
+                run_last[c] = n - k * NT;
+                continue;
+            }
             for (int e = off[n]; e < off[n + 1]; ++e) {
                 const int t = ent[e] / 6, slot = ent[e] % 6;
                 const int li = (int)(std::lower_bound(L0, L1, t) - L0);
@@ -80,23 +90,38 @@ bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, con
                 }
                 L.cent[c].push_back((unsigned short)(slot * 3 * kTile + li % kTile));
                 L.run_end[c].back() += 1;
+                last_c = c;
             }
+            L.run_node[last_c].back() |= kRunFinal;
         }
     }
     L.fixed = tile_record_bytes(mixed);
     L.ns_max = 16;
     L.bytes.assign(C, 0);
+    std::vector<unsigned char> finals;
     for (int k = 0; k < K; ++k) {
+        // Every node of the tile has exactly one final run.
+        const int nn = std::min(N, (k + 1) * NT) - k * NT;
+        finals.assign(nn, 0);
+        for (int c = L.tile_chunk[k]; c < L.tile_chunk[k + 1]; ++c)
+            for (unsigned short u : L.run_node[c])
+                if ((u & kRunFinal) && (u & ~kRunFinal) < nn) finals[u & ~kRunFinal] += 1;
+        for (int j = 0; j < nn; ++j)
+            if (finals[j] != 1) {
+                err = "node tile chunk fails its bounds";
+                return false;
+            }
         for (int c = L.tile_chunk[k]; c < L.tile_chunk[k + 1]; ++c) {
             const long long first = L.start[k] + (long long)(c - L.tile_chunk[k]) * kTile;
             const int ntri = (int)std::max<long long>(0, std::min<long long>(kTile, L.start[k + 1] - first));
             const size_t R = L.run_node[c].size(), E = L.cent[c].size();
-            // What the kernel indexes: entries inside the chunk's live slots,
-            // run nodes inside the tile's accumulators, run ends ascending up
-            // to E, everything inside one record.
-            bool ok = R <= 6 * kTile && E <= 6 * kTile;
+            // What the kernels index: entries inside the chunk's live slots,
+            // run nodes among the tile's nodes (so inside its accumulators
+            // and the mesh), run ends ascending up to E, everything inside
+            // one record.
+            bool ok = R <= 6 * kTile + NT && E <= 6 * kTile;
             for (size_t r = 0; ok && r < R; ++r)
-                ok = L.run_node[c][r] < NT && L.run_end[c][r] > (r ? L.run_end[c][r - 1] : 0);
+                ok = (L.run_node[c][r] & ~kRunFinal) < nn && L.run_end[c][r] >= (r ? L.run_end[c][r - 1] : 0);
             ok = ok && (R == 0 ? E == 0 : L.run_end[c][R - 1] == E);
             for (size_t e = 0; ok && e < E; ++e)
                 ok = L.cent[c][e] / (3 * kTile) < 6 && L.cent[c][e] % (3 * kTile) < ntri;
@@ -115,6 +140,7 @@ bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, con
 
 bool choose_node_tiles(const int* patch_ids, int N, int T, int mixed, int sms, int target, int nt_max, int nt_min,
                        const std::vector<int>& off, const std::vector<int>& ent,
+                       const std::function<size_t(size_t, int)>& smem_for,
                        const std::function<int(size_t)>& blocks_for, NodeTileLayout& L, int& NT, int& blocks,
                        std::string& err) {
     blocks = 0;
@@ -124,7 +150,7 @@ bool choose_node_tiles(const int* patch_ids, int N, int T, int mixed, int sms, i
         NT = std::max(std::min(nt_max, nt_min), (int)((N + k * slots - 1) / (k * slots)));
         L = NodeTileLayout();
         if (!node_tile_layout(patch_ids, N, T, NT, mixed, off, ent, L, err)) return false;
-        const size_t smem = node_tile_smem(L.stride, NT, mixed);
+        const size_t smem = smem_for(L.stride, NT);
         blocks = smem > 227 * 1024 ? 0 : blocks_for(smem);
         if (blocks >= target) break;
         nt_max = nt_max * 7 / 8;

@@ -132,7 +132,7 @@ __device__ __forceinline__ void node_tile_walk(const NodeTilePlan& q, int N, boo
             const unsigned short* re = rn + hd.x;
             const unsigned short* en = re + hd.x;
             for (int r = i; r < hd.x; r += kTile) {
-                const int j = rn[r];
+                const int j = rn[r] & ~kRunFinal;
                 int e = r ? re[r - 1] : 0;
                 const int e1 = re[r];
                 double a0 = acc[3 * j], a1 = acc[3 * j + 1], a2 = acc[3 * j + 2];

@@ -68,6 +68,90 @@ def _dp(a):
     return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def read_settings_file(path: str) -> dict:
+    """``name = value;`` lines of a settings file (read_settings.cpp:47-264's
+    format) as a dict of floats (booleans as 0/1)."""
+    out = {}
+    with open(path) as f:
+        for line in f:
+            line = line.split("//")[0].strip()
+            if "=" not in line or not line.endswith(";"):
+                continue
+            k, v = (x.strip() for x in line[:-1].split("=", 1))
+            out[k] = {"true": 1.0, "false": 0.0}.get(v, None)
+            if out[k] is None:
+                out[k] = float(v)
+    return out
+
+
+class _NS:
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+class RefSetup:
+    """A workload set up by the reference's own code alone
+    (``ref_setup_full``: read_settings, read_vtk_data, calc_mesh_info,
+    set_up_patch_fitting, calc_dof_masses, the scales, timestep and dialling
+    schedule, perturb_node_positions_with_noise; main.cpp:91-209), in the
+    shape ``Oracle`` takes (num_nodes, num_tris, tables(), dofs(), scalars,
+    params), so that a reference run maps no library of this project."""
+
+    def __init__(self, settings_path: str, vtk_path: str, num_nodes: int, num_tris: int):
+        if not available("ref"):
+            raise RuntimeError("reference build absent (python oracle/build.py --reference DIR)")
+        L = _load("ref")
+        d = C.POINTER(C.c_double)
+        u8 = C.POINTER(C.c_uint8)
+        f = L.ref_setup_full
+        f.argtypes = [C.c_char_p, C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int32), d, d, d,
+                      d, d, d, d, d, u8, u8, C.c_char_p, C.c_int]
+        N, T = num_nodes, num_tris
+        self.num_nodes, self.num_tris = N, T
+        patch = np.zeros((T, 6), np.int32)
+        mat2 = np.zeros((T, 18))
+        mass, dofs0, scal = np.zeros(N), np.zeros(3 * N), np.zeros(14)
+        ref_pos = np.zeros((N, 3))
+        area, thick, shear = np.zeros(T), np.zeros(T), np.zeros(T)
+        fixed, boundary = np.zeros(N, np.uint8), np.zeros(N, np.uint8)
+        err = C.create_string_buffer(512)
+        n, t = C.c_int(), C.c_int()
+        rc = f(settings_path.encode(), vtk_path.encode(), C.byref(n), C.byref(t),
+               patch.ctypes.data_as(C.POINTER(C.c_int32)), _dp(mat2), _dp(mass), _dp(dofs0), _dp(scal),
+               _dp(ref_pos), _dp(area), _dp(thick), _dp(shear), fixed.ctypes.data_as(u8),
+               boundary.ctypes.data_as(u8), err, 512)
+        if rc != 0:
+            raise RuntimeError("reference set-up failed: %s" % err.value.decode(errors="replace"))
+        if (n.value, t.value) != (N, T):
+            raise RuntimeError("reference set-up read %d nodes / %d triangles, expected %d / %d"
+                               % (n.value, t.value, N, T))
+        coeffs = np.zeros((T, 24))
+        coeffs[:, 6:] = mat2  # the reference builds its first-derivative weights itself (calc_deriv_mats)
+        self._tables = {"patch_ids": patch, "deriv_coeffs": coeffs, "node_mass": mass, "ref_area": area,
+                        "ref_thickness": thick, "ref_shear_modulus": shear, "is_constrained": fixed,
+                        "is_boundary": boundary}
+        self._flat = ref_pos.T.reshape(-1).copy()
+        self._dofs0 = dofs0
+        st = read_settings_file(settings_path)
+        self.scalars = _NS(min_ref_thickness=scal[2], char_force_scale=scal[3], char_speed_scale=scal[4],
+                           damping_factor_1=scal[6], timestep=scal[7], timesteps_per_dial_phase=int(scal[8]),
+                           timesteps_between_equil_checks=int(scal[9]), damping_factor_2=scal[13],
+                           dial_factors_to_hold_at_spacing=st["dial_factors_to_hold_at_spacing"])
+        self.params = _NS(def_poisson_ratio=st["def_poisson_ratio"],
+                          bend_stiffening_scale_factor=st["bend_stiffening_scale_factor"],
+                          ref_density=st["ref_density"], min_ref_thickness=scal[2], char_force_scale=scal[3],
+                          char_speed_scale=scal[4],
+                          force_to_char_force_ratio_equil_threshold=st["force_to_char_force_ratio_equil_threshold"],
+                          speed_to_char_speed_ratio_equil_threshold=st["speed_to_char_speed_ratio_equil_threshold"])
+
+    def tables(self) -> dict:
+        return self._tables
+
+    def dofs(self, which: int = 1) -> np.ndarray:
+        """SoA dofs: 0 the flat reference state, 1 after the initial noise."""
+        return (self._flat if which == 0 else self._dofs0).copy()
+
+
 class Oracle:
     """One CPU oracle instance over a ``morphoshell_b200.Model``'s tables."""
 

@@ -1,15 +1,19 @@
 """Build recipe of the CPU oracles (TEST INFRASTRUCTURE ONLY).
 
-    python oracle/build.py [--force]
+    python oracle/build.py [--force] [--reference DIR]
 
 1. ``oracle/lib/libmorpho_oracle.so`` -- this project's C++/OpenMP
    restatement of the reference's per-step algorithm (morpho_oracle.cpp).
-2. When the reference tree is present (``/root/reference/source_files``, or
-   ``$MORPHOSHELL_REFERENCE``), the reference's own C++ files compiled
+2. When a reference tree is given (``--reference DIR`` or
+   ``$MORPHOSHELL_REFERENCE``; DIR holds ``source_files/``) and present,
+   the reference's own C++ files compiled
    unmodified with g++ against ``oracle/eigen_shim`` (Eigen 3 is not installed
    here), outputs only under ``oracle/_ref/``:
      _ref/libmorpho_ref.so     every source file except main.cpp, plus
-                               ref_bridge.cpp (the ref_* C ABI of oracle.h)
+                               ref_bridge.cpp (the ref_* C ABI of oracle.h),
+                               plus do_dialling.cpp once more per dialling
+                               protocol 2..5 with that protocol's block
+                               switched on (edit applied in memory)
      _ref/morphoshell_ref      the reference's whole executable, as shipped
                                (dialling protocol 1)
      _ref/morphoshell_ref_p3   the same with do_dialling.cpp's protocol-3 block
@@ -33,7 +37,6 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_DIR = os.path.join(HERE, "lib")
 REF_OUT = os.path.join(HERE, "_ref")
 SHIM = os.path.join(HERE, "eigen_shim")
-REF_SRC = os.environ.get("MORPHOSHELL_REFERENCE", "/root/reference") + "/source_files"
 CXX = ["g++", "-std=c++17", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-w"]
 
 PORT_LIB = os.path.join(LIB_DIR, "libmorpho_oracle.so")
@@ -61,14 +64,16 @@ def build_port(force=False) -> str:
     return PORT_LIB
 
 
-def protocol3_source(text: str) -> str:
-    """do_dialling.cpp with protocol 1 commented out and the protocol-3
-    block (between the comment lines that open and close it) uncommented."""
+def protocol_source(text: str, k: int) -> str:
+    """do_dialling.cpp with protocol 1 commented out and the protocol-k
+    block (k = 2..5, between the comment lines that open and close it)
+    uncommented, the way the reference expects a user to select a protocol
+    (do_dialling.cpp:70-73)."""
     lines = text.split("\n")
     out = []
     p1 = ("abar_comps = (1.0-dial_factor) * a_comps_at_zero_dial_factor + dial_factor * abar_info;",
           "bbar_comps = (1.0-dial_factor) * b_comps_at_zero_dial_factor + dial_factor * bbar_info;")
-    marker = next(i for i, l in enumerate(lines) if l.strip() == "// 3)")
+    marker = next(i for i, l in enumerate(lines) if l.strip() == "// %d)" % k)
     opener = max(i for i in range(marker) if lines[i].strip() == "/*")
     closer = next(i for i in range(marker, len(lines)) if lines[i].strip() == "*/")
     n_p1 = 0
@@ -85,14 +90,29 @@ def protocol3_source(text: str) -> str:
     return "\n".join(out)
 
 
-def build_ref(force=False):
-    if not os.path.isdir(REF_SRC):
+def protocol3_source(text: str) -> str:
+    return protocol_source(text, 3)
+
+
+def reference_sources(reference=None):
+    """source_files/ of the reference tree named by the argument or by
+    $MORPHOSHELL_REFERENCE, or None when neither names an existing tree."""
+    root = reference or os.environ.get("MORPHOSHELL_REFERENCE")
+    if not root:
+        return None
+    src = os.path.join(root, "source_files")
+    return src if os.path.isdir(src) else None
+
+
+def build_ref(force=False, reference=None):
+    ref_src = reference_sources(reference)
+    if ref_src is None:
         return None
     obj_dir = os.path.join(REF_OUT, "obj")
     os.makedirs(obj_dir, exist_ok=True)
     shim_hdrs = [os.path.join(SHIM, "Eigen", h) for h in ("Dense", "Sparse")]
-    srcs = sorted(glob.glob(os.path.join(REF_SRC, "*.cpp")))
-    inc = ["-I" + SHIM, "-I" + REF_SRC]
+    srcs = sorted(glob.glob(os.path.join(ref_src, "*.cpp")))
+    inc = ["-I" + SHIM, "-I" + ref_src]
 
     def comp(src):
         obj = os.path.join(obj_dir, os.path.basename(src)[:-4] + ".o")
@@ -102,12 +122,16 @@ def build_ref(force=False):
 
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         objs = list(ex.map(comp, srcs))
-    p3_obj = os.path.join(obj_dir, "do_dialling_protocol3.o")
-    dd = os.path.join(REF_SRC, "do_dialling.cpp")
-    if force or not _newer(p3_obj, dd, *shim_hdrs):
-        with open(dd) as f:
-            text = protocol3_source(f.read())
-        _run(CXX + inc + ["-Ddo_dialling=do_dialling_protocol3", "-x", "c++", "-c", "-", "-o", p3_obj], stdin=text)
+    dd = os.path.join(ref_src, "do_dialling.cpp")
+    proto_objs = []
+    for k in (2, 3, 4, 5):
+        pk_obj = os.path.join(obj_dir, "do_dialling_protocol%d.o" % k)
+        if force or not _newer(pk_obj, dd, *shim_hdrs):
+            with open(dd) as f:
+                text = protocol_source(f.read(), k)
+            _run(CXX + inc + ["-Ddo_dialling=do_dialling_protocol%d" % k, "-x", "c++", "-c", "-", "-o", pk_obj],
+                 stdin=text)
+        proto_objs.append(pk_obj)
     p3_main_obj = os.path.join(obj_dir, "do_dialling_p3_as_default.o")
     if force or not _newer(p3_main_obj, dd, *shim_hdrs):
         with open(dd) as f:
@@ -119,7 +143,7 @@ def build_ref(force=False):
         _run(CXX + inc + ["-c", bridge, "-o", bridge_obj])
     main_obj = os.path.join(obj_dir, "main.o")
     dd_obj = os.path.join(obj_dir, "do_dialling.o")
-    lib_objs = [o for o in objs if o != main_obj] + [p3_obj, bridge_obj]
+    lib_objs = [o for o in objs if o != main_obj] + proto_objs + [bridge_obj]
     if force or not _newer(REF_LIB, *lib_objs):
         _run(CXX + ["-shared", "-o", REF_LIB] + lib_objs)
     if force or not _newer(REF_EXE, *objs):
@@ -130,15 +154,16 @@ def build_ref(force=False):
     return REF_LIB
 
 
-def build(force=False):
+def build(force=False, reference=None):
     port = build_port(force)
-    ref = build_ref(force)
+    ref = build_ref(force, reference)
     return port, ref
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--reference", default=None, help="reference tree (holds source_files/)")
     a = ap.parse_args()
-    print(build(a.force))
+    print(build(a.force, a.reference))
     sys.exit(0)

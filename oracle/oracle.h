@@ -51,6 +51,14 @@ extern "C" {
 ORACLE_API(orc)
 ORACLE_API(ref)
 
+/* The reference's own set-up (main.cpp:91-209) from a settings file and a
+ * mesh file; ref_* only. */
+int ref_setup_from_files(const char* settings, const char* vtk, int* N_out, int* T_out, int32_t* patch,
+                         double* mat2, double* masses, double* dofs0, double* scal, char* err, int len);
+int ref_setup_full(const char* settings, const char* vtk, int* N_out, int* T_out, int32_t* patch, double* mat2,
+                   double* masses, double* dofs0, double* scal, double* ref_pos, double* area, double* thick,
+                   double* shear, uint8_t* fixed, uint8_t* boundary, char* err, int len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -47,20 +47,25 @@
 #include "is_at_equilibrium.hpp"
 #include "oracle.h"
 
-// do_dialling.cpp compiled a second time with its protocol-3 block enabled
-// (the reference selects protocols by editing that file).
-void do_dialling_protocol3(Eigen::Matrix<double, Eigen::Dynamic, 3>& abar_comps,
-                           Eigen::Matrix<double, Eigen::Dynamic, 3>& bbar_comps,
-                           Eigen::Matrix<double, Eigen::Dynamic, 1>& def_thicknesses,
-                           Eigen::Matrix<double, Eigen::Dynamic, 1>& def_shear_moduli, double dial_factor,
-                           const Eigen::Matrix<double, Eigen::Dynamic, Eigen::Dynamic>& abar_info,
-                           const Eigen::Matrix<double, Eigen::Dynamic, Eigen::Dynamic>& bbar_info,
-                           const Eigen::Matrix<double, Eigen::Dynamic, 3>& a_comps_at_zero_dial_factor,
-                           const Eigen::Matrix<double, Eigen::Dynamic, 3>& b_comps_at_zero_dial_factor,
-                           const std::vector<Tri_Class>& triangles, const std::vector<Node_Class>& nodes,
-                           const Eigen::Matrix<double, Eigen::Dynamic, 1>& dofs,
-                           const Eigen::Matrix<double, Eigen::Dynamic, 3>& normals, Out_Stream_Class& log,
-                           const Stuff_Class& stuff);
+// do_dialling.cpp compiled once more per protocol 2..5 with that protocol's
+// block enabled (the reference selects protocols by editing that file).
+#define MS_DECLARE_DIALLING(NAME)                                                                               \
+    void NAME(Eigen::Matrix<double, Eigen::Dynamic, 3>& abar_comps,                                             \
+              Eigen::Matrix<double, Eigen::Dynamic, 3>& bbar_comps,                                             \
+              Eigen::Matrix<double, Eigen::Dynamic, 1>& def_thicknesses,                                        \
+              Eigen::Matrix<double, Eigen::Dynamic, 1>& def_shear_moduli, double dial_factor,                   \
+              const Eigen::Matrix<double, Eigen::Dynamic, Eigen::Dynamic>& abar_info,                           \
+              const Eigen::Matrix<double, Eigen::Dynamic, Eigen::Dynamic>& bbar_info,                           \
+              const Eigen::Matrix<double, Eigen::Dynamic, 3>& a_comps_at_zero_dial_factor,                      \
+              const Eigen::Matrix<double, Eigen::Dynamic, 3>& b_comps_at_zero_dial_factor,                      \
+              const std::vector<Tri_Class>& triangles, const std::vector<Node_Class>& nodes,                    \
+              const Eigen::Matrix<double, Eigen::Dynamic, 1>& dofs,                                             \
+              const Eigen::Matrix<double, Eigen::Dynamic, 3>& normals, Out_Stream_Class& log,                   \
+              const Stuff_Class& stuff);
+MS_DECLARE_DIALLING(do_dialling_protocol2)
+MS_DECLARE_DIALLING(do_dialling_protocol3)
+MS_DECLARE_DIALLING(do_dialling_protocol4)
+MS_DECLARE_DIALLING(do_dialling_protocol5)
 
 namespace {
 
@@ -89,12 +94,13 @@ void copy_rowmajor(MatXX& m, const double* src, int rows, int cols) {
 }
 
 void dial(Ctx& c, double f) {
-    if (c.protocol == 3)
-        do_dialling_protocol3(c.abar, c.bbar, c.thick, c.shear, f, c.abar_info, c.bbar_info, c.a0, c.b0, c.tris,
-                              c.nodes, c.dofs, c.normals, c.log, c.stuff);
-    else
-        do_dialling(c.abar, c.bbar, c.thick, c.shear, f, c.abar_info, c.bbar_info, c.a0, c.b0, c.tris, c.nodes,
-                    c.dofs, c.normals, c.log, c.stuff);
+    auto* fn = c.protocol == 2   ? &do_dialling_protocol2
+               : c.protocol == 3 ? &do_dialling_protocol3
+               : c.protocol == 4 ? &do_dialling_protocol4
+               : c.protocol == 5 ? &do_dialling_protocol5
+                                 : &do_dialling;
+    fn(c.abar, c.bbar, c.thick, c.shear, f, c.abar_info, c.bbar_info, c.a0, c.b0, c.tris, c.nodes, c.dofs,
+       c.normals, c.log, c.stuff);
 }
 
 }  // namespace
@@ -114,6 +120,18 @@ void ref_set_threads(int n) { omp_set_num_threads(n); }
 // Returns 0, or 1 with the exception text in err (len bytes).
 int ref_setup_from_files(const char* settings, const char* vtk, int* N_out, int* T_out, int32_t* patch,
                          double* mat2, double* masses, double* dofs0, double* scal, char* err, int len) {
+    return ref_setup_full(settings, vtk, N_out, T_out, patch, mat2, masses, dofs0, scal, nullptr, nullptr, nullptr,
+                          nullptr, nullptr, nullptr, err, len);
+}
+
+// As ref_setup_from_files, plus what ref_create needs besides: the flat
+// reference positions as read from the mesh file (N x 3 row-major), per
+// triangle ref_area, ref_thickness and ref_shear_modulus (T each, from
+// calc_mesh_info and read_vtk_data), and per node is_constrained and
+// is_boundary (N each).  Any output may be NULL.
+int ref_setup_full(const char* settings, const char* vtk, int* N_out, int* T_out, int32_t* patch, double* mat2,
+                   double* masses, double* dofs0, double* scal, double* ref_pos, double* area, double* thick,
+                   double* shear, uint8_t* fixed, uint8_t* boundary, char* err, int len) {
     try {
         Stuff_Class st;
         Out_Stream_Class log;
@@ -144,7 +162,19 @@ int ref_setup_from_files(const char* settings, const char* vtk, int* N_out, int*
         calc_timestep(st, log);
         calc_steps_between_outputs(st, log);
         calc_dialling_procedure_params(st, log);
+        if (ref_pos)
+            for (int n = 0; n < st.num_nodes; ++n)
+                for (int k = 0; k < 3; ++k) ref_pos[3 * (size_t)n + k] = P(n, k);
         perturb_node_positions_with_noise(P, st);
+        for (int t = 0; t < st.num_tris; ++t) {
+            if (area) area[t] = tris[t].ref_area;
+            if (thick) thick[t] = tris[t].ref_thickness;
+            if (shear) shear[t] = tris[t].ref_shear_modulus;
+        }
+        for (int n = 0; n < st.num_nodes; ++n) {
+            if (fixed) fixed[n] = nodes[n].is_constrained ? 1 : 0;
+            if (boundary) boundary[n] = nodes[n].is_boundary ? 1 : 0;
+        }
         if (N_out) *N_out = st.num_nodes;
         if (T_out) *T_out = st.num_tris;
         for (int t = 0; t < st.num_tris; ++t) {
@@ -267,8 +297,10 @@ void ref_destroy(void* p) { delete static_cast<Ctx*>(p); }
 int ref_set_programmed(void* p, int protocol, const double* ai, int ka, const double* bi, int kb, double spacing,
                        int from_ansatz) {
     Ctx& c = *static_cast<Ctx*>(p);
-    if (protocol != 1 && protocol != 3) return 8;  // only these two are compiled from the reference
-    if (protocol == 1 && (ka != 3 || kb != 3)) return 1;
+    if (protocol < 1 || protocol > 5) return 8;
+    // Protocols 1 and 2 combine whole T x 3 matrices; 3..5 read columns.
+    const int need_a[6] = {0, 3, 3, 3, 13, 1};
+    if ((protocol <= 2 && (ka != 3 || kb != 3)) || ka < need_a[protocol]) return 1;
     c.protocol = protocol;
     copy_rowmajor(c.abar_info, ai, c.stuff.num_tris, ka);
     copy_rowmajor(c.bbar_info, bi, c.stuff.num_tris, kb);

@@ -68,3 +68,32 @@ def rel_err(a, b):
     a = np.asarray(a)
     b = np.asarray(b)
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def protocol_inputs(model, protocol, seed=0):
+    """(abar_info, bbar_info, dial_factors_to_hold_at_spacing) for a
+    dialling protocol of do_dialling.cpp on a model's mesh: 1 and 2 final
+    abar/bbar (T x 3 each); 3 the LCE director angle, lambda_final and nu_ot;
+    4 eleven lambda checkpoints at dial factors 0, 0.1, ..., 1 then nu_ot and
+    the director angle (T x 13, spacing 0.1, do_dialling.cpp:128-153); 5 the
+    radial coordinate of the centroid (do_dialling.cpp:158-177)."""
+    from morphoshell_b200 import meshgen
+    info, _ = model.programmed()
+    T = model.num_tris
+    rng = np.random.default_rng(seed)
+    if protocol in (1, 2):
+        return meshgen.lce_abar_comps(info, 1.0), 0.3 * rng.standard_normal((T, 3)), 0.05
+    if protocol == 3:
+        return info, np.zeros((T, 1)), 0.05
+    if protocol == 4:
+        lam_final = 0.8 + 0.4 * rng.random(T)
+        k = np.arange(11) / 10.0
+        wobble = 0.02 * rng.standard_normal((T, 11))
+        wobble[:, 0] = 0.0
+        lam = 1.0 + np.outer(lam_final - 1.0, k) + wobble
+        return np.column_stack([lam, np.full(T, 0.5), info[:, 0]]), np.zeros((T, 1)), 0.1
+    x = model.dofs(0).reshape(3, -1)
+    tri = model.tables()["patch_ids"][:, :3]
+    cx, cy = x[0][tri].mean(1), x[1][tri].mean(1)
+    return np.sqrt(cx * cx + cy * cy).reshape(-1, 1), np.zeros((T, 1)), 0.05
+

@@ -4,6 +4,7 @@ from __future__ import annotations
 
 import json
 import os
+import socket
 import subprocess
 import sys
 
@@ -52,8 +53,11 @@ def test_reference_arm_under_torchrun_prints_one_line():
     """Launched as the multi-GPU bench is (torchrun, two ranks), the reference
     arm runs on rank 0 alone and prints exactly one JSON line."""
     env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    with socket.socket(socket.AF_INET, socket.SOCK_STREAM) as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
-           "127.0.0.1", "--master-port", "29631", "bench.py", "--impl", "reference", "--gpus", "2",
+           "127.0.0.1", "--master-port", str(port), "bench.py", "--impl", "reference", "--gpus", "2",
            "--workload", "disk50", "--steps", "3", "--warmup", "3"]
     out = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600, env=env)
     assert out.returncode == 0, out.stderr[-2000:]

@@ -160,3 +160,35 @@ def test_batch_node_tiles_bitwise(tmp_path, precision):
     assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
     for i in range(3):
         assert np.array_equal(out[0][2][i][0], out[1][2][i][0]) and np.array_equal(out[0][2][i][1], out[1][2][i][1])
+
+
+def test_batch_members_against_oracle(tmp_path):
+    """Batch members against the CPU oracle, not only against the
+    single-mesh driver: each instance's dialling trajectory (protocol 3,
+    dialled in-kernel from the instance's own field, step k at
+    dial_factors_to_hold_at_spacing * k / timesteps_per_dial_phase,
+    main.cpp:478-488) after the same number of steps, positions within 1e-9
+    relative.  Step 0 is dialled in-kernel too and lambda^(-2 nu_ot) comes
+    from the device pow, the two places the batch can differ from the
+    reference's do_dialling (do_dialling.cpp:112-123)."""
+    from morphoshell_b200 import MS_INST_DIALLING, Batch
+    from oracle import Oracle
+    models, _ = _members(tmp_path, [15, 16, 17], spacing_range=(0.05, 0.08))
+    n = min(3000, min(m.scalars.timesteps_per_dial_phase for m in models) - 1)
+    b = Batch(models)
+    assert b.run(n) == n
+    for i, m in enumerate(models):
+        st = b.status(i)
+        assert st.status == MS_INST_DIALLING and st.stepcount == n
+        s = m.scalars
+        a_info, b_info = m.programmed()
+        o = Oracle("orc", m)
+        o.set_programmed(3, a_info, b_info, s.dial_factors_to_hold_at_spacing)
+        o.upload(m.dofs(1))
+        dials = s.dial_factors_to_hold_at_spacing * (np.arange(n) / s.timesteps_per_dial_phase)
+        rc, done = o.step_n(n, dials, s.timestep, s.damping_factor_1)
+        assert rc == 0 and done == n
+        ox, ov = o.download()
+        bx, bv = b.download(i)
+        assert np.abs(bx - ox).max() <= 1e-9 * np.abs(ox).max(), i
+        assert np.abs(bx - m.dofs(1)).max() > 0

@@ -1,0 +1,135 @@
+"""Parity at the benchmarked size: 10^4 fixed dialling steps of the
+1.8M-triangle disk on the GPU against the reference's own code.
+
+The reference's run is too long to repeat here (about half an hour of CPU on
+all host threads), so it is a committed fixture, tests/golden/disk1p8m_traj.npz,
+written by tests/golden/make_cfg2_trajectory.py from the reference's own
+per-step functions (compiled from its source).  The fixture holds a seeded
+sample of 65,536 nodes of the final state, the global maxima of the last step
+(max |F|, max |v| and their nodes) and the largest |z| with its node; the
+test first checks that it rebuilt the same mesh, set-up and initial noise
+(a fingerprint of both).
+
+Bars: node positions within 1e-9 relative (norm-wise over the sample, max
+|dx| / max |x| over all nodes) after 10^4 steps, on the node-tiled step and
+on the two-kernel step; the global maxima within 1e-9 relative with the same
+nodes; per-step deformation forces within 1e-12 relative against the CPU
+oracle on the same state at step 0 and at step 10^4.  The mixed-precision
+path is run on the same steps and its error against the reference is
+stated and bounded by the shape-error bar of 1e-5 of the mesh size.
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIXTURE = os.path.join(HERE, "golden", "disk1p8m_traj.npz")
+FORCE_RTOL = 1e-12
+POS_RTOL = 1e-9
+MIXED_SHAPE_TOL = 1e-5  # of the mesh size (diameter 2)
+
+
+@pytest.fixture(scope="module")
+def cfg2(tmp_path_factory):
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    from make_cfg2_trajectory import dial_schedule, fingerprint, sample_nodes
+    from morphoshell_b200 import Model, meshgen
+    g = np.load(FIXTURE)
+    d = str(tmp_path_factory.mktemp("cfg2"))
+    st, vtk = meshgen.write_workload(d, "disk1p8m")
+    m = Model(st, vtk, quiet=True)
+    fp = fingerprint(m)
+    ref_fp = g["fingerprint"]
+    assert fp[:3].tolist() == ref_fp[:3].tolist(), "mesh differs from the fixture's"
+    np.testing.assert_allclose(fp[3:], ref_fp[3:], rtol=1e-13, atol=0)
+    idx = sample_nodes(m.num_nodes)
+    assert np.array_equal(idx, g["sample"])
+    dials = dial_schedule(m.scalars, int(g["steps"]))
+    return m, g, idx, dials
+
+
+def _run(m, dials, precision=0, path=None):
+    from morphoshell_b200 import GpuLoop
+    s = m.scalars
+    a_info, b_info = m.programmed()
+    gl = GpuLoop(m, precision=precision)
+    if path is not None:
+        gl.set_step_path(path)
+    gl.set_programmed(3, a_info, b_info, s.dial_factors_to_hold_at_spacing)
+    gl.upload(m.dofs(1))
+    rep = gl.step_n(len(dials), dials, s.timestep, s.damping_factor_1, check_last=True)
+    return gl, rep
+
+
+def _sample(x, idx, N):
+    return np.stack([x[idx], x[N + idx], x[2 * N + idx]])
+
+
+def _force_err(m, gl, x, v, dial):
+    from oracle import Oracle
+    s = m.scalars
+    a_info, b_info = m.programmed()
+    o = Oracle("orc", m, threads=os.cpu_count())
+    o.set_programmed(3, a_info, b_info, s.dial_factors_to_hold_at_spacing)
+    for t in (gl, o):
+        t.upload(x, v)
+        t.surface_derivs()
+        t.do_dialling(dial)
+    gf, _ = gl.deformation_forces()
+    of, _ = o.deformation_forces()
+    o.close()
+    return rel_err(gf, of)
+
+
+@pytest.mark.parametrize("path", [3, 2])
+def test_cfg2_1e4_steps_against_reference(cfg2, path):
+    m, g, idx, dials = cfg2
+    N = m.num_nodes
+    gl, rep = _run(m, dials, path=path)
+    x, v = gl.download()
+    assert np.isfinite(x).all()
+    dx = np.abs(_sample(x, idx, N) - g["x"]).max()
+    moved = np.abs(g["x"] - _sample(m.dofs(1), idx, N)).max()
+    print("path %d after %d steps: max position difference %.3e (%.3e of max |x|, %.3e of the largest "
+          "displacement %.3e)" % (path, len(dials), dx, dx / g["abs_max"][0], dx / moved, moved))
+    assert dx / g["abs_max"][0] < POS_RTOL
+    assert dx < 1e-3 * moved  # the displacement itself is reproduced to 1e-3 of its size or better
+    # global maxima over all nodes (is_at_equilibrium.cpp:62-90): of the last
+    # step's forces (the check the fused step made) and of the final
+    # velocities; and the largest out-of-plane displacement
+    f_max, v_max, f_node, v_node = g["equil"]
+    assert abs(rep.equil.max_force - f_max) <= POS_RTOL * f_max
+    assert rep.equil.max_force_node == int(f_node)
+    speed = np.sqrt(v[:N] ** 2 + v[N:2 * N] ** 2 + v[2 * N:] ** 2)
+    assert abs(speed.max() - v_max) <= POS_RTOL * v_max
+    assert int(np.argmax(speed)) == int(v_node)
+    z = x[2 * N:]
+    zn, zv = int(g["zmax"][0]), g["zmax"][1]
+    assert int(np.argmax(np.abs(z))) == zn
+    assert abs(z[zn] - zv) <= POS_RTOL * g["abs_max"][0]
+    # per-step forces against the oracle on the state reached, and at step 0
+    assert _force_err(m, gl, x, v, float(dials[-1])) < FORCE_RTOL
+    if path == 3:
+        assert _force_err(m, gl, m.dofs(1), None, float(dials[0])) < FORCE_RTOL
+    gl.close()
+
+
+def test_cfg2_mixed_precision_error_against_reference(cfg2):
+    """The mixed path over the same 10^4 steps: final positions against the
+    reference's, as a fraction of the mesh size (the unit disk, diameter 2)."""
+    m, g, idx, dials = cfg2
+    N = m.num_nodes
+    gl, _ = _run(m, dials, precision=1)
+    x, _ = gl.download()
+    gl.close()
+    shape_err = np.abs(_sample(x, idx, N) - g["x"]).max() / 2.0
+    print("mixed vs reference after %d steps: max position error %.3e of the mesh size" % (len(dials), shape_err))
+    assert shape_err < MIXED_SHAPE_TOL

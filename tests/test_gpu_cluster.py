@@ -124,18 +124,65 @@ def test_mixed_precision_force_error(workdir):
     assert np.abs(forces[1] - forces[0]).max() / cf < 6e-6
 
 
+def test_mixed_precision_force_error_against_oracle(workdir):
+    """The mixed path's per-step force (recovered from one velocity update)
+    against the FP64 oracle's forces on the same state
+    (calc_deformation_forces.cpp:185 + calc_non_deformation_forces.cpp +
+    impose_constraints.cpp), norm-wise."""
+    from morphoshell_b200 import MS_PRECISION_MIXED
+    from oracle import Oracle
+    m = make_model(workdir, "disk18k")
+    s = m.scalars
+    a_info, b_info = m.programmed()
+    mass = np.tile(m.tables()["node_mass"], 3)
+    x, v = deformed_state(m, seed=24, amp=0.02)
+    g, = _loops(m, [1], precision=MS_PRECISION_MIXED)
+    g.upload(x, v)
+    g.step_n(1, np.array([0.5]), s.timestep, 0.0)
+    _, v1 = g.download()
+    mixed = (v1 - v) * mass / s.timestep
+    o = Oracle("orc", m)
+    o.set_programmed(3, a_info, b_info, s.dial_factors_to_hold_at_spacing)
+    o.upload(x, v)
+    o.surface_derivs()
+    o.do_dialling(0.5)
+    o.deformation_forces()
+    o.non_deformation_forces(0.0)
+    o.impose_constraints()
+    err = rel_err(mixed, o.forces())
+    print("mixed-precision force error against the FP64 oracle: %.3e (norm-wise)" % err)
+    assert err < 1.5e-6, err
+
+
 def test_mixed_precision_equilibrium_shape(workdir):
     """Both precisions run the whole dialling schedule to the final
-    equilibrium; shapes agree to well within 1e-5 of the mesh size (1)."""
+    equilibrium; shapes agree to well within 1e-5 of the mesh size (1), and
+    the elastic energy of the mixed path's equilibrium, evaluated by the
+    FP64 oracle (calc_energies.cpp:44-63), is within 1e-4 of the FP64
+    path's (itself pinned to the oracle step by step)."""
     from morphoshell_b200 import MS_PRECISION_MIXED
+    from oracle import Oracle
     m = make_model(workdir, "disk100", dial_factors_to_hold_at_spacing=0.5, dial_phase_time_prefactor=0.02,
                    force_to_char_force_ratio_equil_threshold=1e-5, speed_to_char_speed_ratio_equil_threshold=1e-4)
-    shapes = []
+    s = m.scalars
+    a_info, b_info = m.programmed()
+    shapes, energies = [], []
     for prec in (0, MS_PRECISION_MIXED):
         r, x = m.run(max_steps=3_000_000, precision=prec)
         assert r.final_dial_factor == 1.0 and r.equilibria_reached >= 2, (r.final_dial_factor, r.equilibria_reached)
         shapes.append(x)
-    assert np.abs(shapes[1] - shapes[0]).max() < 1e-5
+        o = Oracle("orc", m)
+        o.set_programmed(3, a_info, b_info, s.dial_factors_to_hold_at_spacing)
+        o.upload(x)
+        o.do_dialling(1.0)
+        e = o.output_quantities()["energies"]
+        energies.append(e[0] + e[1])
+    shape_err = np.abs(shapes[1] - shapes[0]).max()
+    energy_err = abs(energies[1] - energies[0]) / abs(energies[0])
+    print("mixed-precision equilibrium: shape error %.3e of the mesh size, elastic energy error %.3e"
+          % (shape_err, energy_err))
+    assert shape_err < 1e-5
+    assert energy_err < 1e-4
 
 
 @pytest.mark.parametrize("precision", [0, 1])

@@ -1,10 +1,10 @@
-"""The node-tiled one-kernel step (ms_set_step_path 3) against the two-kernel
-step -- GPU.
+"""The node-tiled one-kernel steps (ms_set_step_path 3, and 4 with
+warp-specialised roles) against the two-kernel step -- GPU.
 
-Path 3 computes each triangle with the same arithmetic as the bulk-copy
-per-triangle kernel and sums every node's contributions in ascending
-triangle order from zero, as the node kernel does, so both give the same
-bits (calc_deformation_forces.cpp:185 is the sum both restate)."""
+Paths 3 and 4 compute each triangle with the same arithmetic as the
+bulk-copy per-triangle kernel and sum every node's contributions in
+ascending triangle order from zero, as the node kernel does, so all give
+the same bits (calc_deformation_forces.cpp:185 is the sum they restate)."""
 from __future__ import annotations
 
 import os
@@ -42,15 +42,16 @@ def _run(gs, x, v, m, dial_steps=300, wait_steps=200, check=True):
     return reps
 
 
+@pytest.mark.parametrize("path", [3, 4])
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("name", ["disk18k", "disk100"])
-def test_node_tiles_equal_two_kernel_bitwise(workdir, precision, name):
+def test_node_tiles_equal_two_kernel_bitwise(workdir, precision, name, path):
     """Dialling steps (protocol 3 in-kernel) and waiting steps (programmed
     tensors from memory): identical positions, velocities and equilibrium
     maxima, both precisions; disk100 is a single tile."""
     m = make_model(workdir, name)
     x, v = deformed_state(m, seed=31, amp=0.02)
-    g2, g3 = _loops(m, [2, 3], precision=precision)
+    g2, g3 = _loops(m, [2, path], precision=precision)
     r2, r3 = _run((g2, g3), x, v, m)
     x2, v2 = g2.download()
     x3, v3 = g3.download()
@@ -58,7 +59,7 @@ def test_node_tiles_equal_two_kernel_bitwise(workdir, precision, name):
     e2, e3 = r2.equil, r3.equil
     assert (e2.max_force, e2.max_speed, e2.max_force_node, e2.max_speed_node) == \
         (e3.max_force, e3.max_speed, e3.max_force_node, e3.max_speed_node)
-    assert g3.plan_info()["path"] == 3
+    assert g3.plan_info()["path"] == path
 
 
 def test_node_tiles_other_protocol_bitwise(workdir):
@@ -71,9 +72,11 @@ def test_node_tiles_other_protocol_bitwise(workdir):
     a_info = meshgen.lce_abar_comps(info, 1.0)
     b_info = 0.3 * np.random.default_rng(1).standard_normal((T, 3))
     x, v = deformed_state(m, seed=32, amp=0.02)
-    g2, g3 = _loops(m, [2, 3], protocol=1, a_info=a_info, b_info=b_info)
-    _run((g2, g3), x, v, m, dial_steps=150, wait_steps=50)
-    assert all(np.array_equal(a, b) for a, b in zip(g2.download(), g3.download()))
+    g2, g3, g4 = _loops(m, [2, 3, 4], protocol=1, a_info=a_info, b_info=b_info)
+    _run((g2, g3, g4), x, v, m, dial_steps=150, wait_steps=50)
+    ref = g2.download()
+    for g in (g3, g4):
+        assert all(np.array_equal(a, b) for a, b in zip(ref, g.download()))
 
 
 def test_node_tiles_nonuniform_material_and_field(workdir, tmp_path):
@@ -92,9 +95,11 @@ def test_node_tiles_nonuniform_material_and_field(workdir, tmp_path):
                           shear_modulus=1 + 0.3 * rng.random(T))
     x, v = deformed_state(m, seed=33, amp=0.02)
     for prec in (0, 1):
-        g2, g3 = _loops(m, [2, 3], precision=prec)
-        _run((g2, g3), x, v, m, dial_steps=120, wait_steps=40)
-        assert all(np.array_equal(a, b) for a, b in zip(g2.download(), g3.download()))
+        g2, g3, g4 = _loops(m, [2, 3, 4], precision=prec)
+        _run((g2, g3, g4), x, v, m, dial_steps=120, wait_steps=40)
+        ref = g2.download()
+        for g in (g3, g4):
+            assert all(np.array_equal(a, b) for a, b in zip(ref, g.download()))
 
 
 def test_node_tiles_guard(workdir):
@@ -107,21 +112,23 @@ def test_node_tiles_guard(workdir):
     bad = x.copy()
     bad[2 * m.num_nodes + 4321] += 1e6
     offs = []
-    for g in _loops(m, [2, 3]):
+    for g in _loops(m, [2, 3, 4]):
         g.upload(bad, v)
         with pytest.raises(MsError) as ei:
             g.step_n(10, None, s.timestep, s.damping_factor_2)
         offs.append((ei.value.report.error_step, ei.value.report.offending_dof, ei.value.report.offending_force))
         gx, _ = g.download()
         assert np.array_equal(gx, bad)
-    assert offs[0] == offs[1] and offs[0][0] == 0
+    assert offs[0] == offs[1] == offs[2] and offs[0][0] == 0
 
 
-def test_node_tiles_kernel_timing(workdir):
-    """ms_time_kernels reports the one kernel of path 3 and no node kernel."""
+@pytest.mark.parametrize("path", [3, 4])
+def test_node_tiles_kernel_timing(workdir, path):
+    """ms_time_kernels reports the one kernel of paths 3 and 4 and no node
+    kernel."""
     m = make_model(workdir, "disk18k")
     s = m.scalars
-    (g,) = _loops(m, [3])
+    (g,) = _loops(m, [path])
     x, v = deformed_state(m, seed=35, amp=0.02)
     g.upload(x, v)
     t_tri, t_node = g.time_kernels(5, 0.2, s.timestep, s.damping_factor_1)

@@ -8,10 +8,12 @@ reference compiled from source (tests/test_oracle_pin.py, tests/golden/).
 """
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 
-from conftest import deformed_state, make_model, rel_err
+from conftest import deformed_state, make_model, protocol_inputs, rel_err
 
 FORCE_RTOL = 1e-12
 POS_RTOL = 1e-9
@@ -80,37 +82,46 @@ def test_advance_dynamics(workdir):
     assert rel_err(gv, ov) < 1e-12
 
 
-@pytest.mark.parametrize("protocol", [1, 2, 3, 5])
+@pytest.mark.parametrize("protocol", [1, 2, 3, 4, 5])
 def test_dialling_protocols(workdir, protocol):
-    from morphoshell_b200 import GpuLoop, meshgen
+    """do_dialling.cpp's protocols (4: lambda interpolated between eleven
+    per-triangle checkpoints, do_dialling.cpp:128-153), from the reference
+    state and from an ansatz, against the oracle."""
+    from morphoshell_b200 import GpuLoop
     from oracle import Oracle
     m = make_model(workdir, "disk100")
-    info, _ = m.programmed()
     T = m.num_tris
-    if protocol in (1, 2):
-        a_info = meshgen.lce_abar_comps(info, 1.0)
-        rng = np.random.default_rng(protocol)
-        b_info = 0.3 * rng.standard_normal((T, 3))
-    elif protocol == 3:
-        a_info, b_info = info, np.zeros((T, 1))
-    else:
-        a_info = 0.9 * np.random.default_rng(5).random((T, 1))
-        b_info = np.zeros((T, 1))
+    a_info, b_info, spacing = protocol_inputs(m, protocol)
     g, o = GpuLoop(m), Oracle("orc", m)
     rng = np.random.default_rng(7)
     a0 = np.column_stack([1 + 0.1 * rng.random(T), 0.05 * rng.random(T), 1 + 0.1 * rng.random(T)])
     b0 = 0.1 * rng.standard_normal((T, 3))
     for from_ansatz in (False, True):
         for t in (g, o):
-            t.set_programmed(protocol, a_info, b_info, 0.1, from_ansatz)
+            t.set_programmed(protocol, a_info, b_info, spacing, from_ansatz)
             t.set_zero_dial_state(a0, b0)
-        for dial in (0.0, 0.3, 0.55, 1.0):
+        for dial in (0.0, 0.3, 0.55, 0.97, 1.0):
             g.do_dialling(dial)
             o.do_dialling(dial)
             ga, gb = g.programmed()
             oa, ob = o.programmed()
             assert rel_err(ga, oa) < 1e-14, (protocol, from_ansatz, dial)
             assert np.abs(gb - ob).max() <= 1e-14 * max(1.0, np.abs(ob).max())
+
+
+def test_a_b_normals(workdir):
+    """calc_a_comps_and_b_comps_and_normals.cpp:27-62 (the metric a, the
+    second fundamental form b and the unit normal of every triangle), as
+    called at step 0 when dialling from an ansatz (main.cpp:320-329)."""
+    m, g, o, x, v = _pair(workdir, "disk18k")
+    g.surface_derivs()
+    o.surface_derivs()
+    ga, gb, gn = g.a_b_normals()
+    oa, ob, on = o.a_b_normals()
+    assert rel_err(ga, oa) < 1e-14
+    assert rel_err(gb, ob) < 1e-12
+    assert rel_err(gn, on) < 1e-14
+    assert np.allclose(np.linalg.norm(gn, axis=1), 1.0, atol=1e-14)
 
 
 def test_fused_step_matches_per_function_path(workdir):
@@ -140,32 +151,65 @@ def test_fused_step_matches_per_function_path(workdir):
     assert rel_err(v1, v2) < 1e-10
 
 
-@pytest.mark.parametrize("path", [2, 3])
-def test_fused_steps_vs_oracle_1e4(workdir, path):
+_trajectories = {}
+
+
+def _oracle_trajectory(workdir, name, n):
+    """The oracle's state after n dialling steps from the noisy flat start
+    (step k dials to dial_factors_to_hold_at_spacing * k /
+    timesteps_per_dial_phase, main.cpp:478-488), with its final forces;
+    computed once per mesh."""
+    from oracle import Oracle
+    if (name, n) not in _trajectories:
+        m = make_model(workdir, name)
+        s = m.scalars
+        a_info, b_info = m.programmed()
+        dials = s.dial_factors_to_hold_at_spacing * (np.arange(n) / s.timesteps_per_dial_phase)
+        o = Oracle("orc", m, threads=os.cpu_count())
+        o.set_programmed(3, a_info, b_info, s.dial_factors_to_hold_at_spacing)
+        o.upload(m.dofs(1))
+        rc, done = o.step_n(n, dials, s.timestep, s.damping_factor_1)
+        assert rc == 0 and done == n
+        _trajectories[(name, n)] = (o.download(), dials)
+        o.close()
+    return _trajectories[(name, n)]
+
+
+@pytest.mark.parametrize("name,path", [("disk100", 2), ("disk100", 3), ("disk18k", 2), ("disk18k", 3)])
+def test_fused_steps_vs_oracle_1e4(workdir, name, path):
     """10^4 fused dialling steps from the flat, noisy initial state against the
     oracle, on the two-kernel and on the node-tiled step: node positions
-    within 1e-9 relative."""
+    within 1e-9 relative.  disk18k is the 18k-triangle disk with its own
+    settings (azimuthal director, lambda 1 -> 0.9, 20 dial phases, h = 0.01,
+    nu = 0.5).  Forces on the state reached are compared too: the GPU's
+    deformation forces on the GPU's final state against the oracle's on the
+    same state, within 1e-12."""
     from morphoshell_b200 import GpuLoop
     from oracle import Oracle
-    m = make_model(workdir, "disk100")
+    m = make_model(workdir, name)
     s = m.scalars
     a_info, b_info = m.programmed()
-    x0 = m.dofs(1)
     n = 10000
-    k = np.arange(n)
-    dials = s.dial_factors_to_hold_at_spacing * (k / s.timesteps_per_dial_phase)
-    g, o = GpuLoop(m), Oracle("orc", m)
+    (ox, ov), dials = _oracle_trajectory(workdir, name, n)
+    g = GpuLoop(m)
     g.set_step_path(path)
-    for t in (g, o):
-        t.set_programmed(3, a_info, b_info, s.dial_factors_to_hold_at_spacing)
-        t.upload(x0)
+    g.set_programmed(3, a_info, b_info, s.dial_factors_to_hold_at_spacing)
+    g.upload(m.dofs(1))
     g.step_n(n, dials, s.timestep, s.damping_factor_1)
-    rc, done = o.step_n(n, dials, s.timestep, s.damping_factor_1)
-    assert rc == 0 and done == n
     gx, gv = g.download()
-    ox, ov = o.download()
-    assert rel_err(gx, ox) < POS_RTOL
     assert np.isfinite(gx).all()
+    assert rel_err(gx, ox) < POS_RTOL
+    assert np.abs(gx - m.dofs(1)).max() > 0  # it moved
+    # per-step forces on the state the dynamics reached
+    o = Oracle("orc", m, threads=os.cpu_count())
+    o.set_programmed(3, a_info, b_info, s.dial_factors_to_hold_at_spacing)
+    for t in (g, o):
+        t.upload(gx, gv)
+        t.surface_derivs()
+        t.do_dialling(dials[-1])
+    gf, _ = g.deformation_forces()
+    of, _ = o.deformation_forces()
+    assert rel_err(gf, of) < FORCE_RTOL
 
 
 def test_bitwise_determinism(workdir):

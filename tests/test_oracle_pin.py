@@ -20,10 +20,12 @@ import tempfile
 import numpy as np
 import pytest
 
-from conftest import deformed_state, make_model, rel_err
+from conftest import deformed_state, make_model, protocol_inputs, rel_err
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
+# The per-function golden vectors (make_golden.py); disk1p8m_traj.npz is the
+# GPU trajectory fixture of tests/test_gpu_cfg2.py.
+GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*_p[0-9].npz")))
 
 
 def _golden_model(g):
@@ -122,31 +124,31 @@ def test_trajectory_1e4_steps_against_reference(workdir):
     assert np.abs(res[0][0] - m.dofs(1)).max() > 0  # it moved
 
 
-def test_protocol1_and_ansatz_dialling_against_reference(workdir):
+@pytest.mark.parametrize("proto", [1, 2, 3, 4, 5])
+def test_dialling_protocols_and_ansatz_dialling_against_reference(workdir, proto):
+    """Every dialling protocol of do_dialling.cpp (the reference's own file,
+    compiled once per protocol with that protocol's block switched on), with
+    and without dialling from an ansatz."""
     _need_ref()
-    from morphoshell_b200 import meshgen
     from oracle import Oracle
     m = make_model(workdir, "disk100")
-    info, _ = m.programmed()
     T = m.num_tris
-    a_info = meshgen.lce_abar_comps(info, 1.0)
-    b_info = 0.3 * np.random.default_rng(0).standard_normal((T, 3))
+    ai, bi, spacing = protocol_inputs(m, proto)
     rng = np.random.default_rng(1)
     a0 = np.column_stack([1 + 0.1 * rng.random(T), 0.05 * rng.random(T), 1 + 0.1 * rng.random(T)])
     b0 = 0.1 * rng.standard_normal((T, 3))
-    for proto, ai, bi in ((1, a_info, b_info), (3, info, np.zeros((T, 1)))):
-        for ansatz in (False, True):
-            o, r = Oracle("orc", m), Oracle("ref", m)
-            for t in (o, r):
-                t.set_programmed(proto, ai, bi, 0.05, ansatz)
-                t.set_zero_dial_state(a0, b0)
-            for dial in (0.0, 0.37, 1.0):
-                o.do_dialling(dial)
-                r.do_dialling(dial)
-                ao, bo = o.programmed()
-                ar, br = r.programmed()
-                assert rel_err(ao, ar) < 1e-15, (proto, ansatz, dial)
-                assert np.abs(bo - br).max() <= 1e-15 * max(1.0, np.abs(br).max())
+    for ansatz in (False, True):
+        o, r = Oracle("orc", m), Oracle("ref", m)
+        for t in (o, r):
+            t.set_programmed(proto, ai, bi, spacing, ansatz)
+            t.set_zero_dial_state(a0, b0)
+        for dial in (0.0, 0.3, 0.37, 0.55, 1.0):
+            o.do_dialling(dial)
+            r.do_dialling(dial)
+            ao, bo = o.programmed()
+            ar, br = r.programmed()
+            assert rel_err(ao, ar) < 1e-15, (proto, ansatz, dial)
+            assert np.abs(bo - br).max() <= 1e-15 * max(1.0, np.abs(br).max())
 
 
 def test_force_guard_against_reference(workdir):

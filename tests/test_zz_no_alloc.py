@@ -1,14 +1,14 @@
 """The allocation-free deformation-forces entry point
 (ms_deformation_forces_noalloc), checked against ms_deformation_forces.
 
-Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
-being captured around it, host frameworks that route all device memory
-through their own pool, and real-time loops that must not allocate once
-started.  They hand in device buffers they already own; the entry point
+Some callers cannot call cudaMalloc: host frameworks that route all device
+memory through their own pool, and real-time loops that must not allocate
+once started.  They hand in device buffers they already own; the entry point
 works in a fixed scratch array inside the library.  Because every call
-reuses that array, the test makes two calls in a row on different states and
-compares each with the handle-based entry point, at the force tolerance of
-the other parity tests.
+reuses that array, the test makes two calls in a row on different states of
+one mesh and then a third on a smaller mesh (stale counts and lists of the
+larger mesh lie beyond its nodes in the scratch), and compares each with the
+handle-based entry point, at the force tolerance of the other parity tests.
 
 The file name makes pytest collect it last, so that a run stopping at the
 first failure has already run every other test.
@@ -65,12 +65,13 @@ def _noalloc(model, x, abar, bbar):
 
 
 def test_noalloc_matches_handle_path_on_two_calls(workdir):
-    m = make_model(workdir, "disk18k")
-    for seed, dial in ((11, 0.4), (12, 0.8)):
+    big = make_model(workdir, "disk18k")
+    small = make_model(workdir, "disk50")
+    for m, seed, dial in ((big, 11, 0.4), (big, 12, 0.8), (small, 13, 0.6)):
         x, v = deformed_state(m, seed=seed)
         ref, abar, bbar = _reference_forces(m, x, v, dial)
         got = _noalloc(m, x, abar, bbar)
-        assert rel_err(got, ref) < FORCE_RTOL, (seed, rel_err(got, ref))
+        assert rel_err(got, ref) < FORCE_RTOL, (m.num_tris, seed, rel_err(got, ref))
 
 
 def test_noalloc_rejects_meshes_beyond_its_scratch():
