@@ -226,10 +226,12 @@ def run_reference(args):
         return 0
     import oracle
     kind = "ref" if oracle.available("ref") else "orc"
+    t0 = time.perf_counter()
     if kind == "ref":
         model, info, bbar = reference_workload(args.workload)
     else:
         model, info, bbar = make_workload(args.workload)
+    setup_s = time.perf_counter() - t0
     cores = os.cpu_count() or 1
     o = oracle.Oracle(kind, model, threads=cores)
     s = model.scalars
@@ -261,6 +263,8 @@ def run_reference(args):
                                   "set_up_patch_fitting, calc_dof_masses, noise)" if kind == "ref" else
                                   "this project's host set-up"},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "setup_s": {"mesh_and_host": setup_s,
+                    "note": "mesh generation, files written, then the reference's own set-up from them"},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -289,7 +293,7 @@ KERNEL_NAMES = {"cluster": ("k_cluster_step", "k_halo_update"), "two-kernel": ("
 PATH_IDS = {"cluster": 0, "two-kernel": 1, "tiles": 2, "node-tiles": 3, "node-pipe": 4}
 
 
-def timed_steps(model, info, bbar, precision, path, args, dials, local, dist, clock=None):
+def timed_steps(model, info, bbar, precision, path, args, dials, local, dist, clock=None, setup=None):
     """One handle at `precision`: W warm-up steps, then K fused steps timed
     with CUDA events on the library's stream (barrier + synchronize on both
     sides, max over ranks), then the per-launch kernel times for the
@@ -300,7 +304,10 @@ def timed_steps(model, info, bbar, precision, path, args, dials, local, dist, cl
     from morphoshell_b200 import MS_PRECISION_FP64, MS_PRECISION_MIXED, GpuLoop
     s = model.scalars
     prec = MS_PRECISION_MIXED if precision == "mixed" else MS_PRECISION_FP64
+    t0 = time.perf_counter()
     g = GpuLoop(model, precision=prec, device=local)
+    if setup is not None:
+        setup["device_s"] = time.perf_counter() - t0
     if path != "auto":
         g.set_step_path(PATH_IDS[path])
     path = {v: k for k, v in PATH_IDS.items()}[g.plan_info()["path"]]
@@ -380,14 +387,17 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
 
+    t0 = time.perf_counter()
     model, info, bbar = make_workload(args.workload)
+    host_setup_s = time.perf_counter() - t0
     s = model.scalars
     T = model.num_tris
     dials = dial_sequence(model, args.warmup + args.steps + 64)
     dt, damp = s.timestep, s.damping_factor_1
     clk = ClockSampler(local)
+    setup = {}
     g, ms_max, kernel_ms, path = timed_steps(model, info, bbar, args.precision, args.path, args, dials, local, dist,
-                                             clock=clk)
+                                             clock=clk, setup=setup)
     value = T * args.steps * world / (ms_max / 1e3)
 
     # End to end through the C ABI with the state on the host every step.
@@ -434,6 +444,9 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": 2 * 24 * N + 8,
                 "d2h_bytes_per_step": 2 * 24 * N + 16, "steps": e2e_steps},
         "clocks": clk.summary(),
+        "setup_s": {"mesh_and_host": host_setup_s, "device": setup.get("device_s"),
+                    "note": "mesh generation + host set-up (Model.from_arrays), then ms_create (tables, plans, "
+                            "uploads)"},
     }
 
     # The other half of the metric: the mixed-precision path on the same mesh,
