@@ -22,8 +22,10 @@
 //   accumulators in shared memory (one thread per run, a run being one
 //   node's entries in ascending triangle order), releases the staging area,
 //   and finishes a node (damping, constraints, equilibrium maxima, force
-//   guard, symplectic Euler; node_core) right after the run that the plan
-//   marks as its last.  Chunks are added in order, so each node's force is
+//   guard, symplectic Euler; node_core) once the run that the plan marks as
+//   its last is added: the node's state is loaded into registers then, and
+//   node_core runs after the next chunk's runs, so the load latency hides
+//   behind that work.  Chunks are added in order, so each node's force is
 //   the sum of its contributions in ascending triangle order from zero --
 //   the order, and so the bits, of every other path.
 //
@@ -52,6 +54,7 @@ using namespace tiles;
 constexpr int kPipeThreads = 384;
 constexpr int kNsSlots = 8;   // node-section slots: a chunk's slot is refilled 8 chunks later
 constexpr int kAggBar = 3;    // named barrier of the aggregation group (1, 2: the math groups)
+constexpr int kDefer = 2;     // final runs per aggregation thread and chunk whose node finish is deferred
 
 // Shared memory: two table buffers, two staging areas, the node-section
 // slots, the tile's per-node accumulators.
@@ -238,14 +241,41 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
         if (i == 0 && pending) bar_wait(&full[w], k & 1);
     } else {
         // ---- aggregation group: every chunk of the block, in order --------
+        // A node whose last run is one of the thread's first kDefer runs of
+        // a chunk is finished one chunk later: its state is loaded into
+        // registers as soon as its force is complete, and node_core runs
+        // after the next chunk's runs, so the loads take no round trip of
+        // their own.  Later final runs of a chunk (more than kDefer x 128
+        // runs) are finished at once.
         double fmax = -1.0, vmax = -1.0;
         int fnode = INT_MAX, vnode = INT_MAX;
+        int dn[kDefer];
+        double dF[kDefer][3];
+        NodeIn din[kDefer];
+#pragma unroll
+        for (int k = 0; k < kDefer; ++k) dn[k] = -1;
+        auto add_run = [&](const R* stage, const unsigned short* re, const unsigned short* en, int r, int j,
+                           double& a0, double& a1, double& a2) {
+            int e = r ? re[r - 1] : 0;
+            const int e1 = re[r];
+            a0 = acc[3 * j];
+            a1 = acc[3 * j + 1];
+            a2 = acc[3 * j + 2];
+            for (; e < e1; ++e) {
+                const R* v = stage + en[e];
+                a0 += (double)v[0];
+                a1 += (double)v[kTile];
+                a2 += (double)v[2 * kTile];
+            }
+        };
         Cursor cur;
         cur.start(q);
+        bool aborted = false;
         for (int g = 0; cur.valid(q); ++g, cur.next(q)) {
             const int w = g & 1;
             if (!group_all(bar_wait(&stage_full[w], (g >> 1) & 1), kAggBar)) {
                 if (i == 0) atomicCAS(&s.err->flag, 0, 5);
+                aborted = true;
                 break;
             }
             const R* stage = reinterpret_cast<const R*>(stages + w * SM::stage);
@@ -255,21 +285,41 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
             const unsigned short* re = rn + nruns;
             const unsigned short* en = re + nruns;
             const int n0 = cur.tile * q.nodes;
-            for (int r = i; r < nruns; r += 128) {
+            int cn[kDefer];
+            double cF[kDefer][3];
+            NodeIn cin[kDefer];
+#pragma unroll
+            for (int k = 0; k < kDefer; ++k) {
+                cn[k] = -1;
+                const int r = i + 128 * k;
+                if (r < nruns) {
+                    const unsigned u = rn[r];
+                    const int j = u & ~kRunFinal;
+                    double a0, a1, a2;
+                    add_run(stage, re, en, r, j, a0, a1, a2);
+                    if (u & kRunFinal) {
+                        // The node's force is complete: clear its
+                        // accumulator for the block's next tile, start
+                        // loading its state, finish it after the next chunk.
+                        acc[3 * j] = acc[3 * j + 1] = acc[3 * j + 2] = 0.0;
+                        cn[k] = n0 + j;
+                        cF[k][0] = a0;
+                        cF[k][1] = a1;
+                        cF[k][2] = a2;
+                        cin[k] = node_load(m, s, sc, n0 + j);
+                    } else {
+                        acc[3 * j] = a0;
+                        acc[3 * j + 1] = a1;
+                        acc[3 * j + 2] = a2;
+                    }
+                }
+            }
+            for (int r = i + 128 * kDefer; r < nruns; r += 128) {
                 const unsigned u = rn[r];
                 const int j = u & ~kRunFinal;
-                int e = r ? re[r - 1] : 0;
-                const int e1 = re[r];
-                double a0 = acc[3 * j], a1 = acc[3 * j + 1], a2 = acc[3 * j + 2];
-                for (; e < e1; ++e) {
-                    const R* v = stage + en[e];
-                    a0 += (double)v[0];
-                    a1 += (double)v[kTile];
-                    a2 += (double)v[2 * kTile];
-                }
+                double a0, a1, a2;
+                add_run(stage, re, en, r, j, a0, a1, a2);
                 if (u & kRunFinal) {
-                    // The node's force is complete: clear its accumulator
-                    // for the block's next tile and finish the node.
                     acc[3 * j] = acc[3 * j + 1] = acc[3 * j + 2] = 0.0;
                     const int n = n0 + j;
                     node_core(m, s, sc, gstep, n, node_load(m, s, sc, n), a0, a1, a2, fmax, fnode, vmax, vnode);
@@ -282,8 +332,25 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
             // This chunk's node-section slot is refilled by a bulk copy later.
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_arrive(&stage_free[w]);
+            // The previous chunk's deferred nodes: their state has landed.
+#pragma unroll
+            for (int k = 0; k < kDefer; ++k) {
+                if (dn[k] >= 0)
+                    node_core(m, s, sc, gstep, dn[k], din[k], dF[k][0], dF[k][1], dF[k][2], fmax, fnode, vmax, vnode);
+                dn[k] = cn[k];
+                dF[k][0] = cF[k][0];
+                dF[k][1] = cF[k][1];
+                dF[k][2] = cF[k][2];
+                din[k] = cin[k];
+            }
             // The next chunk's runs may add to the same nodes.
             group_sync(kAggBar);
+        }
+        if (!aborted) {
+#pragma unroll
+            for (int k = 0; k < kDefer; ++k)
+                if (dn[k] >= 0)
+                    node_core(m, s, sc, gstep, dn[k], din[k], dF[k][0], dF[k][1], dF[k][2], fmax, fnode, vmax, vnode);
         }
         if (sc.check) {
             // Block max/argmax over the aggregation group, then the grid fold.

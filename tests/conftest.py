@@ -97,3 +97,41 @@ def protocol_inputs(model, protocol, seed=0):
     cx, cy = x[0][tri].mean(1), x[1][tri].mean(1)
     return np.sqrt(cx * cx + cy * cy).reshape(-1, 1), np.zeros((T, 1)), 0.05
 
+
+def deformation_forces_of(kind, model, x, v, dial, threads=None):
+    """Deformation forces of a CPU oracle (``orc``: the restatement, ``ref``:
+    the reference's own functions) on a state, protocol-3 dialling at `dial`."""
+    from oracle import Oracle
+    s = model.scalars
+    a_info, b_info = model.programmed()
+    o = Oracle(kind, model, threads=threads)
+    o.set_programmed(3, a_info, b_info, s.dial_factors_to_hold_at_spacing)
+    o.upload(x, v)
+    o.surface_derivs()
+    o.do_dialling(dial)
+    f, _ = o.deformation_forces()
+    o.close()
+    return f
+
+
+def check_forces_to_rounding(model, x, v, dial, gpu_forces, rtol=1e-12, threads=None):
+    """GPU deformation forces on a state against the oracle's: within rtol
+    (norm-wise), or -- on states where the forces are small next to the
+    terms they cancel from (near the flat start a - abar is tiny, and two
+    correct double-precision evaluations differ by about eps |a| / |a - abar|
+    relative) -- no further from the oracle than the reference's own code is
+    (compiled from its source), and within three times that of the
+    reference.  Returns (gpu vs oracle, reference vs oracle, gpu vs
+    reference); the last two are None without the reference build."""
+    import oracle
+    of = deformation_forces_of("orc", model, x, v, dial, threads)
+    e_go = rel_err(gpu_forces, of)
+    if not oracle.available("ref"):
+        assert e_go < rtol, e_go
+        return e_go, None, None
+    rf = deformation_forces_of("ref", model, x, v, dial, threads)
+    e_ro, e_gr = rel_err(rf, of), rel_err(gpu_forces, rf)
+    floor = max(rtol, e_ro)
+    assert e_go <= 2 * floor and e_gr <= 3 * floor, (e_go, e_ro, e_gr)
+    return e_go, e_ro, e_gr
+
