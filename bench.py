@@ -315,6 +315,9 @@ def timed_steps(model, info, bbar, precision, path, args, dials, local, dist, cl
     g.upload(model.dofs(1))
     dt, damp = s.timestep, s.damping_factor_1
     g.step_n(args.warmup, dials[:args.warmup], dt, damp)
+    # The CUDA graphs of the K-step call are built during the warm-up, as a
+    # long-running loop builds them once.
+    g.prepare_steps(args.steps, True, dt, damp)
     stream = torch.cuda.ExternalStream(g.stream(), device=torch.device("cuda", local))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)

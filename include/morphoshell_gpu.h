@@ -190,6 +190,14 @@ ms_status ms_deformation_forces_noalloc(int32_t num_nodes, int32_t num_tris, con
 ms_status ms_step_n(ms_handle* h, int n, const double* dial_factors, int dialling, double timestep,
                     double damping_factor, int using_gradient_descent, int check_last, ms_step_report* report);
 
+/* Builds (captures and instantiates) the CUDA graphs that ms_step_n with
+ * the same n, dialling, timestep, damping, gradient-descent and check_last
+ * arguments would use from the current state buffer, launching nothing, so
+ * that the first such call does not pay for them.  No reference counterpart
+ * (it only moves set-up work out of the timed loop). */
+ms_status ms_prepare_steps(ms_handle* h, int n, int dialling, double timestep, double damping_factor,
+                           int using_gradient_descent, int check_last);
+
 /* ---- output diagnostics (main.cpp:412-436) ------------------------------
  * From the current dofs (recomputes cq).  Any output may be NULL.
  * curvatures T x 2 (Gauss, mean; calc_curvatures.cpp), energy_densities
@@ -236,7 +244,8 @@ ms_status ms_node_tile_plan(ms_handle* h, int* nodes_per_tile, int* tiles, int* 
  * bounds checks ms_create runs: node tiles, chunk records (128 triangle
  * slots each), triangles computed per step (a border triangle once per tile
  * it touches), the largest node section and the record stride in bytes,
- * the record bytes copied per step and the shared memory a block needs.
+ * the record bytes copied per step and the shared memory a block needs
+ * (of the node-tiled step, and of the warp-specialised one).
  * Returns MS_ERR_INVALID_ARGUMENT for bad arguments or lists that fail the
  * checks. */
 typedef struct ms_node_tile_info {
@@ -247,6 +256,8 @@ typedef struct ms_node_tile_info {
     long long record_stride;
     long long bytes_per_step;
     long long shared_bytes;
+    long long sliced_entries;   /* largest sliced staging of a chunk (entries per component) */
+    long long pipe_shared_bytes; /* shared memory a block of the warp-specialised step needs */
 } ms_node_tile_info;
 ms_status ms_node_tile_layout(int num_nodes, int num_tris, const int* patch_ids, int nodes_per_tile, int precision,
                               ms_node_tile_info* out);

@@ -26,7 +26,7 @@ GPU_SYMBOLS = [
     "ms_download_forces", "ms_set_programmed", "ms_set_zero_dial_state", "ms_do_dialling",
     "ms_download_programmed", "ms_surface_derivs", "ms_a_b_normals", "ms_deformation_forces",
     "ms_non_deformation_forces", "ms_impose_constraints", "ms_is_at_equilibrium", "ms_advance_dynamics",
-    "ms_step_n", "ms_output_quantities", "ms_device_info", "ms_stream", "ms_time_kernels",
+    "ms_step_n", "ms_prepare_steps", "ms_output_quantities", "ms_device_info", "ms_stream", "ms_time_kernels",
     "ms_deformation_forces_noalloc", "ms_set_step_path", "ms_plan_info", "ms_node_tile_layout", "ms_node_tile_plan",
     "ms_batch_create", "ms_batch_destroy", "ms_batch_last_error", "ms_batch_run", "ms_batch_status",
     "ms_batch_download_dofs", "ms_batch_upload_dofs", "ms_batch_set_schedule", "ms_batch_get_schedule",
@@ -100,7 +100,8 @@ class msh_run_result(C.Structure):
 class ms_node_tile_info(C.Structure):
     _fields_ = [("tiles", C.c_int), ("chunks", C.c_int), ("tri_tile_pairs", C.c_longlong),
                 ("node_section_max", C.c_longlong), ("record_stride", C.c_longlong),
-                ("bytes_per_step", C.c_longlong), ("shared_bytes", C.c_longlong)]
+                ("bytes_per_step", C.c_longlong), ("shared_bytes", C.c_longlong),
+                ("sliced_entries", C.c_longlong), ("pipe_shared_bytes", C.c_longlong)]
 
 
 class ms_batch_instance(C.Structure):
@@ -159,6 +160,7 @@ def lib() -> C.CDLL:
         L.ms_advance_dynamics.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, P(C.c_int64), d]
         L.ms_step_n.argtypes = [C.c_void_p, C.c_int, d, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
                                 P(ms_step_report)]
+        L.ms_prepare_steps.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int]
         L.ms_output_quantities.argtypes = [C.c_void_p, d, d, d, d, d, d]
         L.ms_device_info.argtypes = [C.c_char_p, C.c_size_t]
         L.ms_deformation_forces_noalloc.argtypes = [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -438,6 +440,12 @@ class GpuLoop:
         self._chk(rc, "step_n")
         return rep
 
+    def prepare_steps(self, n, dialling=True, dt=0.0, damping=0.0, gd=False, check_last=False):
+        """Build the CUDA graphs step_n(n, ...) with these arguments will use,
+        without running any step."""
+        self._chk(lib().ms_prepare_steps(self._h, n, int(dialling), dt, damping, int(gd), int(check_last)),
+                  "prepare_steps")
+
     def set_step_path(self, path: int):
         """0: cluster-tiled step, 1: two-kernel step, 2: two-kernel step with
         the per-triangle tables fed by bulk asynchronous copies, 3: node-tiled
@@ -688,10 +696,10 @@ def run_batch(models, max_steps: int = 0, precision: int = MS_PRECISION_FP64, de
 
 def node_tile_layout(patch_ids, num_nodes: int, nodes_per_tile: int = 1024,
                      precision: int = MS_PRECISION_FP64) -> dict:
-    """Layout of the node-tiled step (step path 3) for a mesh's patch table
-    ([T][6] node ids), computed on the host with the checks ms_create runs:
-    tiles, chunks, triangles computed per step, record sizes, shared memory
-    per block."""
+    """Layout of the node-tiled steps (step paths 3 and 4) for a mesh's patch
+    table ([T][6] node ids), computed on the host with the checks ms_create
+    runs: tiles, chunks, triangles computed per step, record sizes, the
+    sliced staging size and the shared memory per block of each kernel."""
     p = np.ascontiguousarray(patch_ids, dtype=np.int32)
     info = ms_node_tile_info()
     rc = lib().ms_node_tile_layout(int(num_nodes), p.shape[0], p.ctypes.data, int(nodes_per_tile), int(precision),

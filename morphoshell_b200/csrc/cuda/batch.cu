@@ -831,7 +831,7 @@ ms_status ms_batch_create(const ms_batch_instance* inst, int32_t n, int32_t devi
         NodeTileLayout L;
         std::string err;
         int NT = 0, blocks = 0;
-        auto smem_for = [&](size_t stride, int nodes) { return node_tile_smem(stride, nodes, mixed); };
+        auto smem_for = [&](const NodeTileLayout& lay, int nodes) { return node_tile_smem(lay.stride, nodes, mixed); };
         if (!choose_node_tiles(patch6.data(), (int)N, (int)T, mixed, sms, mixed ? MSB_NT_MINB_MIXED : MSB_NT_MINB,
                                mixed ? 1008 : 928, 256, off, ent, smem_for, blocks_for, L, NT, blocks, err))
             return bail(bfail(b, MS_ERR_INVALID_ARGUMENT, err));
@@ -852,6 +852,7 @@ ms_status ms_batch_create(const ms_batch_instance* inst, int32_t n, int32_t devi
             q.nchunks = L.C;
             q.grid = sms * blocks;
             q.stride = L.stride;
+            q.slc = L.slc_max;
             q.rec = d_rec;
             q.tile_chunk = d_tc;
             q.chunk_bytes = d_bytes;

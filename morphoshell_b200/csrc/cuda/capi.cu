@@ -262,9 +262,9 @@ ms_status build_tiles(ms_handle* h, const ms_mesh_desc* d) {
 #endif
 constexpr int kNtNodesMin = 256;
 // Largest nodes per tile of the warp-specialised step (one block per SM): its
-// shared memory holds two table buffers, two staging areas and eight node
-// sections besides the accumulators, and tiles this size leave about 14 % of
-// the triangles on tile borders.
+// shared memory holds two table buffers, two staging areas, eight node
+// sections and the prefetched node state besides the accumulators, and tiles
+// this size leave about 14 % of the triangles on tile borders.
 #ifndef MSB_PIPE_NODES
 #define MSB_PIPE_NODES 1600
 #endif
@@ -287,8 +287,10 @@ ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vecto
     NodeTileLayout L;
     std::string err;
     int NT = 0, blocks = 0, pipe_blocks = 0;
-    auto tile_smem = [&](size_t stride, int nodes) { return node_tile_smem(stride, nodes, mixed); };
-    auto pipe_smem = [&](size_t stride, int nodes) { return node_pipe_smem(stride, nodes, mixed); };
+    auto tile_smem = [&](const NodeTileLayout& lay, int nodes) { return node_tile_smem(lay.stride, nodes, mixed); };
+    auto pipe_smem = [&](const NodeTileLayout& lay, int nodes) {
+        return node_pipe_smem(lay.stride, nodes, lay.slc_max, mixed);
+    };
     auto tile_blocks = [&](size_t smem) {
         int b = 0;
         if (prepare_node_tile_kernels(mixed, smem, &b) != cudaSuccess) {
@@ -305,27 +307,25 @@ ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vecto
         }
         return b;
     };
-    // One plan serves both node-tiled kernels.  Its tiles are sized for the
-    // warp-specialised kernel (path 4, one block per SM) when that kernel
-    // can run, else for the node-tiled kernel (path 3).  MSB_NODE_TILE_PLAN=3
-    // in the environment sizes them for path 3 regardless.
+    // One plan serves both node-tiled kernels.  By default its tiles are
+    // sized for the node-tiled kernel (path 3, the faster on B200) and its
+    // records carry no sliced order, so path 4 is not offered.  With
+    // MSB_NODE_TILE_PLAN=4 in the environment the tiles are sized for the
+    // warp-specialised kernel (path 4, one block per SM) and the records
+    // carry the sliced order it reads; path 3 runs on that plan too.
     const char* plan_env = std::getenv("MSB_NODE_TILE_PLAN");
-    const bool plan3 = plan_env && std::string(plan_env) == "3";
-    if (!plan3) {
+    const bool plan4 = plan_env && std::string(plan_env) == "4";
+    if (plan4) {
         if (!choose_node_tiles(d->patch_ids, N, T, mixed, sms, 1, MSB_PIPE_NODES, kNtNodesMin, off, ent, pipe_smem,
-                               pipe_blocks_for, L, NT, pipe_blocks, err))
+                               pipe_blocks_for, L, NT, pipe_blocks, err, 1))
             return fail(h, MS_ERR_INVALID_ARGUMENT, err);
-        if (pipe_blocks > 0) {
-            blocks = tile_blocks(tile_smem(L.stride, NT));
-        }
+        if (pipe_blocks > 0) blocks = tile_blocks(tile_smem(L, NT));
     }
     if (pipe_blocks <= 0) {
         if (!choose_node_tiles(d->patch_ids, N, T, mixed, sms, node_tile_blocks_target(mixed),
                                mixed ? MSB_NT_NODES_MIXED : MSB_NT_NODES, kNtNodesMin, off, ent, tile_smem, tile_blocks,
-                               L, NT, blocks, err))
+                               L, NT, blocks, err, 0))
             return fail(h, MS_ERR_INVALID_ARGUMENT, err);
-        // The warp-specialised kernel on this plan, where it fits.
-        pipe_blocks = pipe_blocks_for(pipe_smem(L.stride, NT));
     }
     if (blocks <= 0 && pipe_blocks <= 0) {
         h->have_ntiles = false;
@@ -350,6 +350,7 @@ ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vecto
     q.grid = sms * blocks;
     q.grid_pipe = sms * std::min(pipe_blocks, 1);
     q.stride = stride;
+    q.slc = L.slc_max;
     q.rec = d_rec;
     q.tile_chunk = d_tile_chunk;
     q.chunk_bytes = d_bytes;
@@ -366,7 +367,8 @@ ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vecto
     h->have_ntiles = q.grid > 0;
     h->have_pipe = q.grid_pipe > 0;
     // The node-tiled kernels once every block has a tile of its own (same
-    // bits as paths 1 and 2): the warp-specialised one where it runs.
+    // bits as paths 1 and 2); the warp-specialised one when its plan was
+    // asked for.
     if (h->have_pipe && K >= q.grid_pipe) h->step_path = 4;
     else if (h->have_ntiles && K >= q.grid) h->step_path = 3;
     return MS_OK;
@@ -616,7 +618,7 @@ ms_status ms_create(const ms_mesh_desc* d, const ms_params* prm, int device, int
     ms_status st;
     if ((st = dalloc(h, &patch, 6ULL * T)) || (st = dalloc(h, &coef, 24ULL * T)) || (st = dalloc(h, &area, T)) ||
         (st = dalloc(h, &thick, T)) || (st = dalloc(h, &shear, T)) || (st = dalloc(h, &mass, N)) ||
-        (st = dalloc(h, &fixed, N)))
+        (st = dalloc(h, &fixed, N + 4)))
         return bail(st);
     if ((st = upload_transposed<int>(h, patch, d->patch_ids, T, 6)) ||
         (st = upload_transposed<double>(h, coef, d->deriv_coeffs, T, 24)))
@@ -625,7 +627,8 @@ ms_status ms_create(const ms_mesh_desc* d, const ms_params* prm, int device, int
         cudaMemcpy(thick, d->ref_thickness, sizeof(double) * T, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(shear, d->ref_shear_modulus, sizeof(double) * T, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(mass, d->node_mass, sizeof(double) * N, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(fixed, d->is_constrained, N, cudaMemcpyHostToDevice) != cudaSuccess)
+        cudaMemcpy(fixed, d->is_constrained, N, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(fixed + N, 0, 4) != cudaSuccess)  // whole 4-byte words are read around the last nodes
         return bail(MS_ERR_CUDA);
     if (d->is_boundary) {
         if ((st = dalloc(h, &boundary, N))) return bail(st);
@@ -957,6 +960,41 @@ static ms_status stage_dials(ms_handle* h, const double* dials, int n) {
     return MS_OK;
 }
 
+static cudaError_t launch_step(ms_handle* h, const StepScalars& sc, bool cluster, int dial_mode, cudaStream_t st);
+
+// The graph of one chunk of fused steps (key.len steps from buffer
+// key.parity), captured on the handle's stream and cached; the cache keeps
+// the eight most recently used.
+static ms_status capture_steps(ms_handle* h, const GraphKey& key, bool cluster, cudaGraphExec_t* out) {
+    cudaStream_t st = h->stream;
+    cudaGraph_t graph;
+    MS_CUDA(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t ce = cudaSuccess;
+    const int dial_mode = key.dial_mode & 15;
+    for (int i = 0; i < key.len && ce == cudaSuccess; ++i) {
+        StepScalars sc{i, key.parity ^ (i & 1), key.dt, key.damping, h->rho_hh, h->force_limit, key.gd,
+                       (key.check_last && i == key.len - 1) ? 1 : 0};
+        ce = launch_step(h, sc, cluster, dial_mode, st);
+    }
+    if (ce == cudaSuccess) ce = launch_chunk_end(h->s, key.len, st);
+    cudaError_t ee = cudaStreamEndCapture(st, &graph);
+    if (ce != cudaSuccess) return cuda_fail(h, ce, "capture");
+    if (ee != cudaSuccess) return cuda_fail(h, ee, "cudaStreamEndCapture");
+    cudaGraphExec_t exec = nullptr;
+    ee = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ee != cudaSuccess) return cuda_fail(h, ee, "cudaGraphInstantiate");
+    if (h->graphs.size() >= 8) {
+        auto it = std::min_element(h->graphs.begin(), h->graphs.end(),
+                                   [](const GraphEntry& a, const GraphEntry& b) { return a.last_use < b.last_use; });
+        cudaGraphExecDestroy(it->exec);
+        h->graphs.erase(it);
+    }
+    h->graphs.push_back({key, exec, ++h->use_clock});
+    *out = exec;
+    return MS_OK;
+}
+
 // The two kernels of one fused step on the selected path.
 static cudaError_t launch_step(ms_handle* h, const StepScalars& sc, bool cluster, int dial_mode, cudaStream_t st) {
     cudaError_t e;
@@ -1037,28 +1075,7 @@ ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, doub
                 done += len;
                 continue;
             }
-            cudaGraph_t graph;
-            MS_CUDA(h, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-            cudaError_t ce = cudaSuccess;
-            for (int i = 0; i < len && ce == cudaSuccess; ++i) {
-                StepScalars sc{i, key.parity ^ (i & 1), dt, damping, h->rho_hh, h->force_limit, gd,
-                               (key.check_last && i == len - 1) ? 1 : 0};
-                ce = launch_step(h, sc, cluster, dial_mode, st);
-            }
-            if (ce == cudaSuccess) ce = launch_chunk_end(h->s, len, st);
-            cudaError_t ee = cudaStreamEndCapture(st, &graph);
-            if (ce != cudaSuccess) return cuda_fail(h, ce, "capture");
-            if (ee != cudaSuccess) return cuda_fail(h, ee, "cudaStreamEndCapture");
-            ee = cudaGraphInstantiate(&exec, graph, 0);
-            cudaGraphDestroy(graph);
-            if (ee != cudaSuccess) return cuda_fail(h, ee, "cudaGraphInstantiate");
-            if (h->graphs.size() >= 8) {
-                auto it = std::min_element(h->graphs.begin(), h->graphs.end(),
-                                           [](const GraphEntry& a, const GraphEntry& b) { return a.last_use < b.last_use; });
-                cudaGraphExecDestroy(it->exec);
-                h->graphs.erase(it);
-            }
-            h->graphs.push_back({key, exec, ++h->use_clock});
+            MS_TRY(capture_steps(h, key, cluster, &exec));
         }
         MS_CUDA(h, cudaGraphLaunch(exec, st));
         done += len;
@@ -1103,6 +1120,37 @@ ms_status ms_step_n(ms_handle* h, int n, const double* dials, int dialling, doub
     if (rep) {
         rep->steps_done = n;
         if (check_last) fill_equil(h, *h->h_equil, &rep->equil);
+    }
+    return MS_OK;
+}
+
+ms_status ms_prepare_steps(ms_handle* h, int n, int dialling, double dt, double damping, int gd, int check_last) {
+    if (!h || n < 0) return MS_ERR_INVALID_ARGUMENT;
+    if (n == 0) return MS_OK;
+    if (dialling && !h->programmed)
+        return fail(h, MS_ERR_INVALID_ARGUMENT, "dialling steps need ms_set_programmed");
+    const bool fuse_lce = dialling && lce_fusable(h);
+    if (dialling && !fuse_lce) return MS_OK;  // launched step by step, no graph to build
+    const int dial_mode = fuse_lce ? DIAL_LCE : DIAL_ARRAYS;
+    const bool cluster = use_cluster(h, dialling != 0);
+    if (dialling) {
+        // The dial-factor buffer the graphs read must be in place first.
+        std::vector<double> zeros(n, 0.0);
+        MS_TRY(stage_dials(h, zeros.data(), n));
+        MS_CUDA(h, cudaStreamSynchronize(h->stream));
+    }
+    const int p0 = h->cur;
+    for (int done = 0; done < n;) {
+        const int len = std::min(kChunk, n - done);
+        GraphKey key{len, p0 ^ (done & 1), dial_mode + (cluster ? 16 : 0) + 32 * h->step_path, gd,
+                     (check_last && done + len == n) ? 1 : 0, dt, damping};
+        bool have = false;
+        for (auto& g : h->graphs) have = have || g.key == key;
+        if (!have) {
+            cudaGraphExec_t exec;
+            MS_TRY(capture_steps(h, key, cluster, &exec));
+        }
+        done += len;
     }
     return MS_OK;
 }
@@ -1209,6 +1257,9 @@ ms_status ms_node_tile_layout(int num_nodes, int num_tris, const int* patch_ids,
     for (unsigned x : L.bytes) b += x;
     out->bytes_per_step = b;
     out->shared_bytes = (long long)node_tile_smem(L.stride, nodes_per_tile, precision == MS_PRECISION_MIXED);
+    out->sliced_entries = L.slc_max;
+    out->pipe_shared_bytes =
+        (long long)node_pipe_smem(L.stride_sliced, nodes_per_tile, L.slc_max, precision == MS_PRECISION_MIXED);
     return MS_OK;
 }
 

@@ -149,8 +149,16 @@ constexpr int kNtMaxNodes = 32768;
 //   uint16 ent[E]        patch slot * 3 kTile + slot in chunk, per node ascending t
 //                        (the x component of the contribution in the block's
 //                        field-major staging area; y and z follow kTile apart)
-// A block sums a node's contributions run by run, chunk by chunk, so every
-// node's force is the sum in ascending triangle order, as in the node kernel.
+//   uint16 slice_off[S]  the same entries in sliced order, for the
+//                        warp-specialised step: runs 32s .. 32s + 31 form
+//                        slice s (runs go longest first), and entry u of run
+//                        r sits at slice_off[r / 32] + 32 u + r % 32
+//   uint16 dst[6][kTile] for patch slot sl of the chunk's triangle i, the
+//                        sliced position of its contribution (0xFFFF when
+//                        the node is not in the tile)
+// with the header {R, E, ntri, S}.  A block sums a node's contributions run
+// by run, chunk by chunk, so every node's force is the sum in ascending
+// triangle order, as in the node kernel.
 struct NodeTilePlan {
     int nodes;                       // nodes per tile
     int ntiles;
@@ -162,6 +170,7 @@ struct NodeTilePlan {
     const int* tile_chunk;           // [ntiles + 1] first chunk of each tile
     const unsigned* chunk_bytes;     // [nchunks] bytes to copy of each record (multiple of 16)
     const int* chunk_tri;            // [nchunks][kTile] triangle of each slot, -1 past the chunk's end
+    int slc;                         // entries of the sliced staging area (NodeTileLayout::slc_max)
 };
 
 // Host-side layout of a node-tile plan for tiles of NT consecutive nodes
@@ -177,10 +186,17 @@ struct NodeTileLayout {
     std::vector<std::vector<unsigned short>> run_node, run_end, cent;  // per chunk
     std::vector<unsigned> bytes;    // [C] bytes to copy (fixed part + node section)
     size_t fixed = 0, stride = 0, ns_max = 0;
+    std::vector<std::vector<unsigned short>> slice_off, dst;  // per chunk (sliced staging)
+    int slc_max = 0;                // largest sliced staging of a chunk (entries, multiple of 32)
+    bool sliced = false;            // records carry slice_off and dst (the warp-specialised step)
+    size_t stride_sliced = 0;       // the record stride with them
 };
 // off/ent: each node's (6t + slot) entries in ascending order (CSR).
+// sliced: the records carry the sliced order (slice_off, dst) that the
+// warp-specialised step reads; the node-tiled step and the batch do not
+// need it.
 bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, const std::vector<int>& off,
-                      const std::vector<int>& ent, NodeTileLayout& L, std::string& err);
+                      const std::vector<int>& ent, NodeTileLayout& L, std::string& err, int sliced = 0);
 // A block walks its tiles in turn, so a step takes as long as the block with
 // the most tiles: the tile size is chosen (between nt_min and nt_max nodes)
 // so that the tile count is a multiple of sms x target blocks, at the largest
@@ -188,13 +204,13 @@ bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, con
 // sets up the kernel and returns its resident blocks per SM (0 when it
 // cannot run).  On return `blocks` is the resident blocks of the chosen plan
 // (0: the kernel cannot run); false with err for inconsistent lists.
-// smem_for(stride, nodes) is the kernel's shared memory per block for a
+// smem_for(layout, nodes) is the kernel's shared memory per block for a
 // layout.
 bool choose_node_tiles(const int* patch_ids, int N, int T, int mixed, int sms, int target, int nt_max, int nt_min,
                        const std::vector<int>& off, const std::vector<int>& ent,
-                       const std::function<size_t(size_t, int)>& smem_for,
+                       const std::function<size_t(const NodeTileLayout&, int)>& smem_for,
                        const std::function<int(size_t)>& blocks_for, NodeTileLayout& L, int& NT, int& blocks,
-                       std::string& err);
+                       std::string& err, int sliced = 0);
 // The chunk records of a layout (ids from patch_ids [T][6]; weights from
 // coef_d [T][24] double, or coef_f float for the mixed path when given; the
 // trigonometry block from aux4 [T][4] = area, cos^2, sin^2, cos sin, or
@@ -330,7 +346,7 @@ cudaError_t launch_tri_tiles(const DevMesh& m, const ClusterPlan& p, const DevSt
 size_t node_tile_smem(size_t stride, int nodes, int mixed);
 // Warp-specialised node-tiled step (node_pipe.cu): shared memory per block,
 // kernel set-up (resident blocks per SM), launch.
-size_t node_pipe_smem(size_t stride, int nodes, int mixed);
+size_t node_pipe_smem(size_t stride, int nodes, int slc, int mixed);
 cudaError_t prepare_node_pipe_kernels(int mixed, size_t smem, int* blocks_per_sm);
 cudaError_t launch_node_pipe(const DevMesh& m, const ClusterPlan& p, const NodeTilePlan& q, const DevState& s,
                              const StepScalars& sc, int dial_mode, int mixed, cudaStream_t st);

@@ -11,7 +11,7 @@
 namespace msb {
 
 bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, const std::vector<int>& off,
-                      const std::vector<int>& ent, NodeTileLayout& L, std::string& err) {
+                      const std::vector<int>& ent, NodeTileLayout& L, std::string& err, int sliced) {
     if (NT <= 0 || NT > kNtMaxNodes) {
         err = "nodes per tile must be in 1..32768";
         return false;
@@ -95,8 +95,82 @@ bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, con
             L.run_node[last_c].back() |= kRunFinal;
         }
     }
+    // Within a chunk the runs are independent (distinct nodes), so their
+    // order is free: longest first, so that the runs a warp takes together
+    // (one per thread) have similar lengths and no lane waits long for
+    // another.  Each run keeps its entries in ascending t.
+    {
+        std::vector<int> idx;
+        std::vector<unsigned short> rn, re, ce;
+        for (int c = 0; c < C; ++c) {
+            const int R = (int)L.run_node[c].size();
+            idx.resize(R);
+            for (int r = 0; r < R; ++r) idx[r] = r;
+            auto len = [&](int r) { return (int)L.run_end[c][r] - (r ? (int)L.run_end[c][r - 1] : 0); };
+            std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) { return len(a) > len(b); });
+            rn.clear();
+            re.clear();
+            ce.clear();
+            for (int r : idx) {
+                const int e0 = r ? L.run_end[c][r - 1] : 0;
+                for (int e = e0; e < (int)L.run_end[c][r]; ++e) ce.push_back(L.cent[c][e]);
+                rn.push_back(L.run_node[c][r]);
+                re.push_back((unsigned short)ce.size());
+            }
+            L.run_node[c].swap(rn);
+            L.run_end[c].swap(re);
+            L.cent[c].swap(ce);
+        }
+    }
+    // The sliced order of each chunk's entries (the warp-specialised step):
+    // slice s holds runs 32s .. 32s + 31, 32 entries per row, as many rows
+    // as its first (longest) run has entries.
+    L.slice_off.assign(C, {});
+    L.dst.assign(C, {});
+    L.slc_max = 32;
+    for (int c = 0; c < C; ++c) {
+        const auto& re = L.run_end[c];
+        const int R = (int)re.size();
+        auto len = [&](int r) { return (int)re[r] - (r ? (int)re[r - 1] : 0); };
+        std::vector<unsigned short>& so = L.slice_off[c];
+        int off = 0;
+        for (int r = 0; r < R; r += 32) {
+            so.push_back((unsigned short)off);
+            off += 32 * len(r);
+        }
+        if (off >= 65535) {
+            err = "node tile chunk fails its bounds";
+            return false;
+        }
+        L.slc_max = std::max(L.slc_max, (off + 31) / 32 * 32);
+        std::vector<unsigned short>& d = L.dst[c];
+        d.assign(6 * kTile, 0xFFFF);
+        // Every sliced position gets at most one contribution and lies
+        // inside its slice (runs within a slice are no longer than its
+        // first), so no two writes of a chunk collide.
+        std::vector<unsigned char> used(off, 0);
+        for (int r = 0; r < R; ++r) {
+            const int e0 = r ? re[r - 1] : 0;
+            if (len(r) > len(r / 32 * 32)) {
+                err = "node tile chunk fails its bounds";
+                return false;
+            }
+            for (int e = e0; e < (int)re[r]; ++e) {
+                const int ce = L.cent[c][e], sl = ce / (3 * kTile), li = ce % (3 * kTile);
+                const int pos = so[r / 32] + 32 * (e - e0) + r % 32;
+                if (sl >= 6 || li >= kTile || pos >= off || used[pos] || d[sl * kTile + li] != 0xFFFF) {
+                    err = "node tile chunk fails its bounds";
+                    return false;
+                }
+                used[pos] = 1;
+                d[sl * kTile + li] = (unsigned short)pos;
+            }
+        }
+    }
     L.fixed = tile_record_bytes(mixed);
     L.ns_max = 16;
+    L.sliced = sliced != 0;
+    size_t ns_max_sliced = 16;
     L.bytes.assign(C, 0);
     std::vector<unsigned char> finals;
     for (int k = 0; k < K; ++k) {
@@ -129,28 +203,33 @@ bool node_tile_layout(const int* patch_ids, int N, int T, int NT, int mixed, con
                 err = "node tile chunk fails its bounds";
                 return false;
             }
-            const size_t ns = (16 + 4 * R + 2 * E + 15) / 16 * 16;
+            const size_t S = L.slice_off[c].size();
+            const size_t ns_plain = (16 + 4 * R + 2 * E + 15) / 16 * 16;
+            const size_t ns_sliced = (16 + 4 * R + 2 * E + 2 * S + 2 * 6 * kTile + 15) / 16 * 16;
+            const size_t ns = L.sliced ? ns_sliced : ns_plain;
             L.ns_max = std::max(L.ns_max, ns);
+            ns_max_sliced = std::max(ns_max_sliced, ns_sliced);
             L.bytes[c] = (unsigned)(L.fixed + ns);
         }
     }
     L.stride = L.fixed + (L.ns_max + 127) / 128 * 128;
+    L.stride_sliced = L.fixed + (ns_max_sliced + 127) / 128 * 128;
     return true;
 }
 
 bool choose_node_tiles(const int* patch_ids, int N, int T, int mixed, int sms, int target, int nt_max, int nt_min,
                        const std::vector<int>& off, const std::vector<int>& ent,
-                       const std::function<size_t(size_t, int)>& smem_for,
+                       const std::function<size_t(const NodeTileLayout&, int)>& smem_for,
                        const std::function<int(size_t)>& blocks_for, NodeTileLayout& L, int& NT, int& blocks,
-                       std::string& err) {
+                       std::string& err, int sliced) {
     blocks = 0;
     for (int attempt = 0; attempt < 4; ++attempt) {
         const long long slots = (long long)std::max(sms, 1) * target;
         const long long k = std::max(1LL, (N + slots * nt_max - 1) / (slots * nt_max));
         NT = std::max(std::min(nt_max, nt_min), (int)((N + k * slots - 1) / (k * slots)));
         L = NodeTileLayout();
-        if (!node_tile_layout(patch_ids, N, T, NT, mixed, off, ent, L, err)) return false;
-        const size_t smem = smem_for(L.stride, NT);
+        if (!node_tile_layout(patch_ids, N, T, NT, mixed, off, ent, L, err, sliced)) return false;
+        const size_t smem = smem_for(L, NT);
         blocks = smem > 227 * 1024 ? 0 : blocks_for(smem);
         if (blocks >= target) break;
         nt_max = nt_max * 7 / 8;
@@ -193,13 +272,19 @@ void fill_node_tile_records(const NodeTileLayout& L, const int* patch_ids, const
             }
             int32_t* hd = reinterpret_cast<int32_t*>(r + fixed);
             const int R = (int)L.run_node[c].size(), E = (int)L.cent[c].size();
+            const int S = L.sliced ? (int)L.slice_off[c].size() : 0;
             hd[0] = R;
             hd[1] = E;
             hd[2] = ntri;
+            hd[3] = S;
             unsigned short* u = reinterpret_cast<unsigned short*>(r + fixed + 16);
             std::copy(L.run_node[c].begin(), L.run_node[c].end(), u);
             std::copy(L.run_end[c].begin(), L.run_end[c].end(), u + R);
             std::copy(L.cent[c].begin(), L.cent[c].end(), u + 2 * R);
+            if (L.sliced) {
+                std::copy(L.slice_off[c].begin(), L.slice_off[c].end(), u + 2 * R + E);
+                std::copy(L.dst[c].begin(), L.dst[c].end(), u + 2 * R + E + S);
+            }
         }
     }
 }

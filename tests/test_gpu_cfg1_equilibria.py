@@ -13,7 +13,7 @@ committed fixture rather than run here.
 Checked (main.cpp:282-304, 396-438, 478-507; is_at_equilibrium.cpp:92-98;
 write_output.cpp:77-170): equilibria at the same steps and dial factors;
 every equilibrium's positions within 1e-9 of the disk's size; the last
-file's layout and its per-triangle and per-node fields.
+file's layout and its per-triangle and per-node fields within 1e-10 norm-wise.
 """
 from __future__ import annotations
 
@@ -29,7 +29,7 @@ pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
 FIXTURE = os.path.join(HERE, "golden", "disk18k_equilibria.npz")
 POINT_TOL = 1e-9    # of the largest coordinate (the disk's radius)
-FIELD_TOL = 1e-7    # norm-wise per field
+FIELD_TOL = 1e-10   # norm-wise per field (the last equilibrium: 2e-11 measured)
 
 
 def test_cfg1_equilibria_match_reference_executable(tmp_path):

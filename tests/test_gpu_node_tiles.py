@@ -1,5 +1,6 @@
 """The node-tiled one-kernel steps (ms_set_step_path 3, and 4 with
-warp-specialised roles) against the two-kernel step -- GPU.
+warp-specialised roles, on the plan built for it) against the two-kernel
+step -- GPU.
 
 Paths 3 and 4 compute each triangle with the same arithmetic as the
 bulk-copy per-triangle kernel and sum every node's contributions in
@@ -17,15 +18,27 @@ from conftest import deformed_state, make_model
 pytestmark = pytest.mark.gpu
 
 
-def _loops(m, paths, precision=0, protocol=3, a_info=None, b_info=None):
+def new_loop(m, path, precision=0):
+    """A handle whose plan serves `path`: the warp-specialised step (4) needs
+    the plan built for it (MSB_NODE_TILE_PLAN=4 when the handle is made)."""
     from morphoshell_b200 import GpuLoop
+    if path == 4:
+        os.environ["MSB_NODE_TILE_PLAN"] = "4"
+    try:
+        g = GpuLoop(m, precision=precision)
+    finally:
+        os.environ.pop("MSB_NODE_TILE_PLAN", None)
+    g.set_step_path(path)
+    return g
+
+
+def _loops(m, paths, precision=0, protocol=3, a_info=None, b_info=None):
     s = m.scalars
     if a_info is None:
         a_info, b_info = m.programmed()
     out = []
     for p in paths:
-        g = GpuLoop(m, precision=precision)
-        g.set_step_path(p)
+        g = new_loop(m, p, precision)
         g.set_programmed(protocol, a_info, b_info, s.dial_factors_to_hold_at_spacing)
         out.append(g)
     return out
@@ -146,3 +159,23 @@ def test_node_tile_plan_balances_blocks(workdir):
         nt, tiles, blocks = info["nodes_per_tile"], info["node_tiles"], info["node_tile_blocks"]
         assert tiles == -(-m.num_nodes // nt) and 0 < blocks <= tiles
         assert nt == 256 or tiles % blocks == 0 or tiles % blocks > 0.9 * blocks
+
+
+def test_prepared_graphs_give_the_same_steps(workdir):
+    """ms_prepare_steps builds the graphs of a later ms_step_n call and runs
+    nothing: the state is untouched, and the prepared call gives the bits of
+    an unprepared one."""
+    m = make_model(workdir, "disk18k")
+    s = m.scalars
+    x, v = deformed_state(m, seed=36, amp=0.02)
+    dials = 0.2 + 1e-5 * np.arange(40)
+    out = []
+    for prepare in (True, False):
+        (g,) = _loops(m, [3])
+        g.upload(x, v)
+        if prepare:
+            g.prepare_steps(40, True, s.timestep, s.damping_factor_1)
+            assert all(np.array_equal(a, b) for a, b in zip(g.download(), (x, v)))
+        g.step_n(40, dials, s.timestep, s.damping_factor_1)
+        out.append(g.download())
+    assert all(np.array_equal(a, b) for a, b in zip(out[0], out[1]))

@@ -74,3 +74,20 @@ def test_layout_repeated_patch_node():
     P = np.array([[0, 1, 2, 0, 1, 2], [1, 2, 3, 0, 4, 5]], dtype=np.int32)
     info = node_tile_layout(P, 6, 256)
     assert info["tiles"] == 1 and info["chunks"] == 1 and info["tri_tile_pairs"] == 2
+
+
+def test_layout_sliced_order_sizes(workdir):
+    """The sliced staging of the warp-specialised step: whole rows of 32
+    entries, at least a chunk's entries, and the shared memory of its
+    block (two table buffers, two staging areas of three planes, eight node
+    sections, the prefetched node state, the accumulators)."""
+    from morphoshell_b200 import node_tile_layout
+    m = make_model(workdir, "disk18k")
+    P = m.tables()["patch_ids"]
+    for prec in (0, 1):
+        info = node_tile_layout(P, m.num_nodes, 1024, prec)
+        slc = info["sliced_entries"]
+        assert slc % 32 == 0 and slc >= 6 * 128 // 2
+        fixed = 128 * (6 * 4 + 24 * (4 if prec else 8) + 4 * 8)
+        stage = -(-3 * slc * (4 if prec else 8) // 128) * 128
+        assert info["pipe_shared_bytes"] > 2 * fixed + 2 * stage + 2 * 128 * 8 * 8 + 24 * 1024
