@@ -17,6 +17,8 @@ needed between steps.
 ``value``: K * T * N / (max over ranks of the device time of K steps), FP64.
 ``mixed``: the same K steps on the mixed-precision path (FP32 per-triangle
 arithmetic), with its ratio to FP64 and its force error against FP64.
+``time_to_equilibrium``: learned warm start against the plain start on a
+small disk (time_to_equilibrium()).
 ``e2e``: the same metric with the state on the host, through the C ABI, every
 step: pinned host dofs + velocities copied in (ms_upload_dofs), one fused step
 (ms_step_n), dofs + velocities copied back (ms_download_dofs).
@@ -479,12 +481,54 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(model, info, bbar)
     g.close()
+    if rank == 0 and world == 1 and not args.no_warmstart:
+        line["time_to_equilibrium"] = time_to_equilibrium(local)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def time_to_equilibrium(device: int, seed: int = 11) -> dict:
+    """The metric's last part, at a reduced scale: time to the first
+    equilibrium at dial factor 1 from the plain start and from the learned
+    warm start (morphoshell_b200.warmstart).  The plain method's own
+    equilibria of 64 seeded programmed fields (director theta + sum_k a_k
+    sin(k theta + phi_k), lambda ~ U(0.8, 1.2)) on a 0.06-spacing disk train
+    the tensor-core network; 16 held-out fields then run from both starts in
+    one batch each.  Four short dial phases and thresholds 1e-5 / 1e-4 keep
+    it to about a minute (BASELINE configs 4 and 5 ask for 4096 fields on the
+    18k disk and 64 on the 1.8M disk)."""
+    import tempfile as _tf
+
+    from morphoshell_b200 import Mlp, Model, meshgen, warmstart
+    t0 = time.time()
+    d = _tf.mkdtemp(prefix="ms_tte_")
+    st, vtk = meshgen.write_workload(d, "disk60", dial_factors_to_hold_at_spacing=0.25,
+                                     dial_phase_time_prefactor=0.02, force_to_char_force_ratio_equil_threshold=1e-5,
+                                     speed_to_char_speed_ratio_equil_threshold=1e-4)
+    m = Model(st, vtk, quiet=True)
+    train = warmstart.fields(64, seed=seed)
+    held = warmstart.fields(16, seed=seed + 1)
+    finals, _, status, _ = warmstart.solve(m, train)
+    keep = [i for i, s_ in enumerate(status) if s_ == 3]
+    net = Mlp(warmstart.N_FEATURES, width=128, hidden_layers=3, out_dim=3, seed=1, device=device)
+    losses = warmstart.train_network(net, m, [train[i] for i in keep], [finals[i] for i in keep], epochs=300,
+                                     batch=4096, lr=2e-3, rounds=3)
+    r = warmstart.evaluate(net, m, held)
+    net.close()
+    return {"workload": "disk60: %d triangles, %d training fields, %d held out, 4 dial phases of 0.02 long times, "
+                        "thresholds 1e-5 / 1e-4" % (m.num_tris, len(keep), len(held)),
+            "plain_steps_mean": r["plain_steps_mean"], "learned_steps_mean": r["learned_steps_mean"],
+            "step_speedup": r["step_speedup"], "plain_wall_s": r["plain_wall_s"], "learned_wall_s": r["learned_wall_s"],
+            "wall_speedup": r["wall_speedup"], "fell_back": r["fell_back"],
+            "same_shape_fraction": r["same_shape_fraction"],
+            "energy_ratio_learned_to_plain": r["learned_energy_median"] / r["plain_energy_median"],
+            "loss_first_last": [float(losses[0]), float(losses[-1])], "total_s": time.time() - t0,
+            "note": "reduced-scale stand-in for BASELINE configs 4/5; same_shape_fraction is the share of held-out "
+                    "fields whose learned-start equilibrium is the plain-start one"}
 
 
 def run_ensemble(args):
@@ -636,6 +680,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision half of the line")
+    ap.add_argument("--no-warmstart", action="store_true", help="skip the time-to-equilibrium part of the line")
     ap.add_argument("--path", choices=["auto", "cluster", "two-kernel", "tiles", "node-tiles", "node-pipe"],
                     default="auto",
                     help="fused-step implementation (ms_set_step_path); auto: the library's default")
