@@ -248,6 +248,7 @@ def evaluate(net: Mlp, model, flds, precision=MS_PRECISION_FP64, max_steps=2_000
         elif starts[i] is None:
             s_total[i] = s_plain[i]
     dist = [shape_distance(a, b) for a, b in zip(plain, learned)]
+    start_dist = [shape_distance(x, p) for x, p in zip(starts, plain) if x is not None]
     e_plain = [elastic_energy(model, f, x) for f, x in zip(flds, plain)]
     e_learn = [elastic_energy(model, f, x) for f, x in zip(flds, learned)]
     return {
@@ -259,6 +260,7 @@ def evaluate(net: Mlp, model, flds, precision=MS_PRECISION_FP64, max_steps=2_000
         "plain_done": int((st_plain == MS_INST_DONE).sum()), "learned_done": int((st_learn == MS_INST_DONE).sum()),
         "failed": int((st_plain == MS_INST_FAILED).sum() + (st_learn == MS_INST_FAILED).sum()),
         "shape_distance_max": float(np.max(dist)), "shape_distance_median": float(np.median(dist)),
+        "start_distance_median": float(np.median(start_dist)) if start_dist else None,
         "same_shape_fraction": float(np.mean(np.array(dist) < 0.05)),
         "plain_energy_median": float(np.median(e_plain)), "learned_energy_median": float(np.median(e_learn)),
         "learned_lower_energy_fraction": float(np.mean(np.array(e_learn) <= np.array(e_plain))),
