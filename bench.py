@@ -483,6 +483,14 @@ def run_ours(args):
     g.close()
     if rank == 0 and world == 1 and not args.no_warmstart:
         line["time_to_equilibrium"] = time_to_equilibrium(local)
+    if rank == 0 and world == 1 and not args.no_ensemble:
+        # The batched-ensemble workload (256 disks of assorted sizes stepped
+        # together) on the same GPU and precision, after the single-mesh runs
+        # have released their memory.
+        r = ensemble_measurement(256, args.precision, args.warmup, 200, local, None, 1, 0)
+        r["unit"] = METRIC
+        line["ensemble"] = r
+        line["gpu_launches"] += r["gpu_launches"]
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -531,30 +539,20 @@ def time_to_equilibrium(device: int, seed: int = 11) -> dict:
                     "fields whose learned-start equilibrium is the plain-start one"}
 
 
-def run_ensemble(args):
-    """``--workload ensembleN`` (default N = 256): N independent disks in one
-    batch (ms_batch_*), spacing log-uniform in [0.004, 0.02], lambda_final
-    ~ U(0.8, 1.2), defect charge from {+1, -1, +1/2} (director angle =
-    charge * theta), thickness ~ U(0.005, 0.02), seed 7.  Every instance
-    runs its own dialling / equilibrium state machine on the device; the
-    timed steps are ms_batch_run over the whole ensemble.  With N GPUs the
+def ensemble_measurement(n: int, precision: str, warmup: int, steps: int, local: int, dist, world: int,
+                         rank: int) -> dict:
+    """N independent disks in one batch (ms_batch_*) on this rank's GPU,
+    spacing log-uniform in [0.004, 0.02], lambda_final ~ U(0.8, 1.2), defect
+    charge from {+1, -1, +1/2} (director angle = charge * theta), thickness
+    ~ U(0.005, 0.02), seed 7.  Every instance runs its own dialling /
+    equilibrium state machine on the device; the timed steps are
+    ms_batch_run over the whole ensemble after the schedule autotuner
+    (ms_batch_autotune) has chosen the step's kernels.  With N GPUs the
     members are split over the ranks by weight (strong scaling, no
-    collective on the data path)."""
+    collective on the data path).  Returns the figures of one line."""
     import torch
-    from morphoshell_b200 import MS_PRECISION_FP64, MS_PRECISION_MIXED, Batch, ensemble
+    from morphoshell_b200 import MS_PRECISION_FP64, MS_PRECISION_MIXED, Batch, ensemble, meshgen
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800),
-                                device_id=torch.device("cuda", local))
-    n = int(args.workload[len("ensemble"):] or 256)
-    from morphoshell_b200 import meshgen
     # The members are split over the ranks by their triangle counts (about
     # 1 / spacing^2), so the whole ensemble is the workload at every N.
     weights = [1.0 / meshgen.ensemble_params(k, seed=7)["spacing"] ** 2 for k in range(n)]
@@ -565,12 +563,12 @@ def run_ensemble(args):
                                             threads=cores, processes=min(cores, 32))
     setup_s = time.time() - t0
     log("ensemble of %d built in %.1f s" % (n, setup_s))
-    prec = MS_PRECISION_MIXED if args.precision == "mixed" else MS_PRECISION_FP64
+    prec = MS_PRECISION_MIXED if precision == "mixed" else MS_PRECISION_FP64
     b = Batch(models, precision=prec, device=local)
     info = b.info()
     T = info["num_tris"]
     sched, tune_ms = b.autotune(steps_per_trial=8)
-    b.run(args.warmup)
+    b.run(warmup)
     stream = torch.cuda.ExternalStream(b.stream(), device=torch.device("cuda", local))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -579,7 +577,7 @@ def run_ensemble(args):
             dist.barrier()
         torch.cuda.synchronize()
         e0.record(stream)
-        done = b.run(args.steps)
+        done = b.run(steps)
         e1.record(stream)
         torch.cuda.synchronize()
         if dist:
@@ -592,30 +590,62 @@ def run_ensemble(args):
         dist.all_reduce(tt, op=dist.ReduceOp.SUM)
     ms_max = float(t.item())
     value = float(tt.item()) / (ms_max / 1e3)
-    bpt = BYTES_PER_TRI[args.precision]
+    bpt = BYTES_PER_TRI[precision]
     achieved = bpt * T / (ms_max / done / 1e3) / 1e9
     peak, peak_kind = measured_peak_hbm()
     sizes = [p["num_tris"] for p in params]
-    line = {
-        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": done, "warmup": args.warmup,
-        "ms_per_step": ms_max / done, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed", "data": "synthetic",
-        "config": {"workload": "ensemble%d: %d unit disks in one batch per GPU, spacing log-uniform [0.004, 0.02] "
-                               "(%d..%d triangles, %d in all), lambda_final ~ U(0.8, 1.2), charge in "
-                               "{+1, -1, +1/2}, h ~ U(0.005, 0.02), per-instance dialling state machines"
-                               % (n, n, min(sizes), max(sizes), T),
-                   "precision": args.precision, "num_tris": T, "num_nodes": info["num_nodes"],
-                   "instances": n, "schedule": sched, "autotune_ms_per_step": tune_ms,
-                   "host_setup_s": setup_s, "parallelism": "members split over %d GPUs" % world,
-                   "l2": "inputs far larger than L2; no flush"},
-        "gpu_launches": 4 * done,
+    if sched["tri_block"] < 0:
+        kernels, per_step = "k_batch_pre + k_batch_node_tiles + k_batch_post (node-tiled schedule)", 3
+    elif sched["tri_block"] == 0:
+        kernels, per_step = "k_batch_pre + k_batch_tri_tiles + k_batch_node + k_batch_post (tiled schedule)", 4
+    else:
+        kernels, per_step = "k_batch_pre + k_batch_tri + k_batch_node + k_batch_post (per-thread schedule)", 4
+    b.close()
+    return {
+        "value": value, "steps": done, "ms_per_step": ms_max / done,
+        "workload": "ensemble%d: %d unit disks in one batch per GPU, spacing log-uniform [0.004, 0.02] "
+                    "(%d..%d triangles, %d in all), lambda_final ~ U(0.8, 1.2), charge in "
+                    "{+1, -1, +1/2}, h ~ U(0.005, 0.02), per-instance dialling state machines"
+                    % (n, len(mine), min(sizes), max(sizes), T),
+        "num_tris": T, "num_nodes": info["num_nodes"], "instances": n, "schedule": sched,
+        "autotune_ms_per_step": tune_ms, "host_setup_s": setup_s, "gpu_launches": per_step * done,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_kind": peak_kind,
-                     "kernel": "one step = k_batch_pre + k_batch_tri + k_batch_node + k_batch_post (whole step)",
+                     "traffic": None, "peak_kind": peak_kind, "kernel": kernels + ", whole step",
                      "algorithmic_bytes_per_tri": bpt},
         "clocks": clk.summary(),
     }
-    b.close()
+
+
+def run_ensemble(args):
+    """``--workload ensembleN`` (default N = 256): the batch of N disks that
+    ensemble_measurement describes, as its own line."""
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800),
+                                device_id=torch.device("cuda", local))
+    n = int(args.workload[len("ensemble"):] or 256)
+    r = ensemble_measurement(n, args.precision, args.warmup, args.steps, local, dist, world, rank)
+    line = {
+        "metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": world, "steps": r["steps"],
+        "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed", "data": "synthetic",
+        "config": {"workload": r["workload"], "precision": args.precision, "num_tris": r["num_tris"],
+                   "num_nodes": r["num_nodes"], "instances": n, "schedule": r["schedule"],
+                   "autotune_ms_per_step": r["autotune_ms_per_step"], "host_setup_s": r["host_setup_s"],
+                   "parallelism": "members split over %d GPUs" % world,
+                   "l2": "inputs far larger than L2; no flush"},
+        "gpu_launches": r["gpu_launches"],
+        "roofline": r["roofline"],
+        "clocks": r["clocks"],
+    }
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -681,6 +711,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision half of the line")
     ap.add_argument("--no-warmstart", action="store_true", help="skip the time-to-equilibrium part of the line")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 256-disk batched-ensemble part of the line")
     ap.add_argument("--path", choices=["auto", "cluster", "two-kernel", "tiles", "node-tiles", "node-pipe"],
                     default="auto",
                     help="fused-step implementation (ms_set_step_path); auto: the library's default")

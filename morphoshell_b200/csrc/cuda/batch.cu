@@ -44,6 +44,20 @@ using namespace tridev;
 
 __device__ __forceinline__ bool is_frozen(int status) { return status >= INST_DONE; }
 
+// Material of triangle t of an instance: the instance's uniform material
+// (coefficients formed on the host) or the triangle's own.
+__device__ __forceinline__ void inst_material(const InstParams& q, const DevMesh& m, int t, TriMat<double>& mt) {
+    if (q.uniform_hmu) {
+        mt.h = q.h;
+        mt.mu = q.mu;
+        mt.ks = q.ks;
+        mt.kb = q.kb;
+        mt.igmh = q.igmh;
+    } else {
+        set_material(__ldg(m.thick + t), __ldg(m.shear + t), q.nu, q.gamma, mt);
+    }
+}
+
 __global__ void k_batch_pre(const InstParams* __restrict__ ip, InstState* __restrict__ is, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -86,17 +100,11 @@ __global__ void __launch_bounds__(BLOCK) k_batch_tri(const DevMesh m, const Clus
         const InstState& st = is[inst];
         if (!is_frozen(st.status)) {
             const InstParams& q = ip[inst];
-            double h, mu;
-            if (q.uniform_hmu) {
-                h = q.h;
-                mu = q.mu;
-            } else {
-                h = __ldg(m.thick + t);
-                mu = __ldg(m.shear + t);
-            }
+            TriMat<double> mt;
+            inst_material(q, m, t, mt);
             const int ids[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
             tri_contrib<DIAL_LCE, MIXED>(m, p, pos_buf(s, parity), t, ids, st.cur_dial, st.cur_lam, st.cur_pw, f,
-                                         q.nu, q.gamma, h, mu);
+                                         q.nu, mt);
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -126,13 +134,7 @@ __device__ __forceinline__ void batch_tri(const DevMesh& m, const int* __restric
     if (is_frozen(st.status)) return;
     const InstParams& q = ip[inst];
     TriMat<double> mt;
-    if (q.uniform_hmu) {
-        mt.h = q.h;
-        mt.mu = q.mu;
-    } else {
-        mt.h = __ldg(m.thick + t);
-        mt.mu = __ldg(m.shear + t);
-    }
+    inst_material(q, m, t, mt);
     mt.area = area;
     lce_metric(c2, s2, cs, __dmul_rn(st.cur_lam, st.cur_lam), st.cur_pw, mt);
     double P[6][3];
@@ -142,7 +144,7 @@ __device__ __forceinline__ void batch_tri(const DevMesh& m, const int* __restric
         P[sl][1] = __ldg(pos + m.N + ids[sl]);
         P[sl][2] = __ldg(pos + 2 * m.N + ids[sl]);
     }
-    tri_forces<MIXED>(P, c, mt, q.nu, q.gamma, f);
+    tri_forces<MIXED>(P, c, mt, q.nu, f);
 }
 
 // The same contributions from bulk-copied tile records (tile_copy.cuh),
@@ -179,10 +181,10 @@ __device__ __forceinline__ void batch_node_core(const DevMesh& m, const DevState
     const double* vel = vel_buf(s, parity);
     const double vx = vel[n], vy = vel[N + n], vz = vel[2 * N + n];
     const double mass = __ldg(m.mass + n);
-    const double dm = -damping * mass;
-    Fx += dm * vx / q.rho_hh;
-    Fy += dm * vy / q.rho_hh;
-    Fz += dm * vz / q.rho_hh;
+    const double dm = -damping * mass / q.rho_hh;
+    Fx += dm * vx;
+    Fy += dm * vy;
+    Fz += dm * vz;
     if (__ldg(m.fixed + n)) Fx = Fy = Fz = 0.0;
     if (check) {
         fnorm[n] = sqrt(Fx * Fx + Fy * Fy + Fz * Fz);
@@ -653,6 +655,7 @@ ms_status ms_batch_create(const ms_batch_instance* inst, int32_t n, int32_t devi
         q.gamma = in.params.bend_stiffening_scale_factor;
         q.h = d.ref_thickness[0];
         q.mu = d.ref_shear_modulus[0];
+        dev::material_coefs(q.h, q.mu, q.nu, q.gamma, q.ks, q.kb, q.igmh);
         q.uniform_hmu = 1;
         for (int t = 1; t < Ti && q.uniform_hmu; ++t)
             q.uniform_hmu = d.ref_thickness[t] == q.h && d.ref_shear_modulus[t] == q.mu;

@@ -11,6 +11,7 @@
 
 #include "../../../include/morphoshell_gpu.h"
 #include "internal.cuh"
+#include "tri_physics.cuh"
 
 using namespace msb;
 
@@ -648,6 +649,7 @@ ms_status ms_create(const ms_mesh_desc* d, const ms_params* prm, int device, int
     m.uniform_hmu = uniform ? 1 : 0;
     m.h_uniform = d->ref_thickness[0];
     m.mu_uniform = d->ref_shear_modulus[0];
+    dev::material_coefs(m.h_uniform, m.mu_uniform, m.nu, m.gamma, m.ks_uniform, m.kb_uniform, m.igmh_uniform);
 
     // Incidence lists: node -> (6t + slot), ascending t.
     std::vector<int> off(N + 1, 0), ent(6ULL * T);

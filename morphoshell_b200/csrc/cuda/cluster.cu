@@ -73,9 +73,9 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int ids[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
         const int halo_mask = b.z;
         R f[18];
-        double h, mu;
-        tri_hmu(m, t, h, mu);
-        tri_contrib<DIAL, MIXED>(m, p, pos, t, ids, dial, lam, pw, f, m.nu, m.gamma, h, mu);
+        TriMat<double> mt;
+        tri_material(m, t, mt);
+        tri_contrib<DIAL, MIXED>(m, p, pos, t, ids, dial, lam, pw, f, m.nu, mt);
         R* dst = ctr + (size_t)k * kStride;
 #pragma unroll
         for (int j = 0; j < 18; ++j) dst[j] = f[j];
@@ -159,9 +159,9 @@ __global__ void __launch_bounds__(kAosBlock, MSB_TRI_MINB)
         const int4 a = __ldg(p.tri_idx + 2 * t);
         const int4 b = __ldg(p.tri_idx + 2 * t + 1);
         const int ids[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
-        double h, mu;
-        tri_hmu(m, t, h, mu);
-        tri_contrib<DIAL, MIXED>(m, p, pos_buf(s, sc.parity), t, ids, dial, lam, pw, f, m.nu, m.gamma, h, mu);
+        TriMat<double> mt;
+        tri_material(m, t, mt);
+        tri_contrib<DIAL, MIXED>(m, p, pos_buf(s, sc.parity), t, ids, dial, lam, pw, f, m.nu, mt);
     } else {
 #pragma unroll
         for (int j = 0; j < 18; ++j) f[j] = R(0);

@@ -85,6 +85,7 @@ struct DevMesh {
     // uniform material (used when uniform_hmu)
     int uniform_hmu;
     double h_uniform, mu_uniform;
+    double ks_uniform, kb_uniform, igmh_uniform;  // dev::material_coefs of the uniform material
     // constants
     double nu, gamma;
     // float contributions of the mixed-precision path (null otherwise)
@@ -245,6 +246,7 @@ struct InstParams {
     double dt, damping1, damping2, rho_hh, force_limit;
     double nu, gamma;
     double h, mu;                  // used when uniform_hmu
+    double ks, kb, igmh;           // dev::material_coefs of (h, mu), used when uniform_hmu
     double char_force, char_speed, force_thresh, speed_thresh;
     double spacing;                // dial_factors_to_hold_at_spacing
     double lam_final, nu_ot;       // protocol-3 field (uniform per instance)

@@ -75,9 +75,13 @@ __device__ __forceinline__ void load_material(const DevMesh& m, int t, TriMat<do
     if (m.uniform_hmu) {
         mt.h = m.h_uniform;
         mt.mu = m.mu_uniform;
+        mt.ks = m.ks_uniform;
+        mt.kb = m.kb_uniform;
+        mt.igmh = m.igmh_uniform;
     } else {
         mt.h = __ldg(m.thick + t);
         mt.mu = __ldg(m.shear + t);
+        dev::material_coefs(mt.h, mt.mu, m.nu, m.gamma, mt.ks, mt.kb, mt.igmh);
     }
     mt.area = __ldg(m.area + t);
 }
@@ -186,7 +190,7 @@ __global__ void k_forces_from_cq(const DevMesh m, const DevState s, int write_dE
     mt.bbar1 = m.bbar[(size_t)m.T + t];
     mt.bbar2 = m.bbar[2 * (size_t)m.T + t];
     CqGrad<double> g;
-    dev::energy_gradient<double>(c, mt, m.nu, m.gamma, g);
+    dev::energy_gradient<double>(c, mt, m.nu, g);
     if (write_dE) {
         double* o = s.dEdcq + (size_t)t * 15;
         o[0] = g.rx.x; o[1] = g.ry.x; o[2] = g.rxx.x; o[3] = g.rxy.x; o[4] = g.ryy.x;
@@ -214,8 +218,8 @@ __global__ void k_gather_forces(const DevMesh m, const DevState s) {
 __global__ void k_damping(const DevMesh m, const DevState s, int parity, double damping, double rho_hh) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.N) return;
-    const double dm = -damping * m.mass[n];
-    for (int c = 0; c < 3; ++c) s.forces[(size_t)c * m.N + n] += dm * vel_buf(s, parity)[(size_t)c * m.N + n] / rho_hh;
+    const double dm = -damping * m.mass[n] / rho_hh;
+    for (int c = 0; c < 3; ++c) s.forces[(size_t)c * m.N + n] += dm * vel_buf(s, parity)[(size_t)c * m.N + n];
 }
 
 __global__ void k_constraints(const DevMesh m, const DevState s) {
@@ -435,7 +439,7 @@ __global__ void k_output_tri(const DevMesh m, const DevState s, double* curv, do
     mt.bbar2 = m.bbar[2 * T + t];
     CqGrad<double> g;
     double ws, wb;
-    dev::energy_gradient<double>(c, mt, m.nu, m.gamma, g, &ws, &wb);
+    dev::energy_gradient<double>(c, mt, m.nu, g, &ws, &wb);
     const double a0 = dev::dot(c.rx, c.rx), a1 = dev::dot(c.rx, c.ry), a2 = dev::dot(c.ry, c.ry);
     const V3<double> cr = dev::cross(c.rx, c.ry);
     const double cn2 = dev::dot(cr, cr);

@@ -182,9 +182,10 @@ __global__ void k_na_tri(Scratch* s, int N, int T, const int* __restrict__ patch
     m.bbar2 = bbar[3 * (size_t)t + 2];
     m.h = thick[t];
     m.mu = shear[t];
+    material_coefs(m.h, m.mu, nu, gamma, m.ks, m.kb, m.igmh);
     m.area = area[t];
     CqGrad<double> g;
-    energy_gradient<double>(q, m, nu, gamma, g);
+    energy_gradient<double>(q, m, nu, g);
     double* o = s->contrib + 18 * (size_t)t;
     for (int k = 0; k < 6; ++k) {
         const double mxx = c[6 + 3 * k], mxy = c[7 + 3 * k], myy = c[8 + 3 * k];

@@ -140,10 +140,11 @@ __device__ __forceinline__ void node_core(const DevMesh& m, const DevState& s, c
     const double vx = in.vx, vy = in.vy, vz = in.vz;
     const double mass = in.mass;
     if (!sc.gd) {
-        const double dm = -sc.damping * mass;
-        Fx += dm * vx / sc.rho_hh;
-        Fy += dm * vy / sc.rho_hh;
-        Fz += dm * vz / sc.rho_hh;
+        // One division per node: -damping m / (rho h^2), then per component.
+        const double dm = -sc.damping * mass / sc.rho_hh;
+        Fx += dm * vx;
+        Fy += dm * vy;
+        Fz += dm * vz;
     }
     if (in.fixed) Fx = Fy = Fz = 0.0;
     if (sc.check) {

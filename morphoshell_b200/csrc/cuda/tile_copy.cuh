@@ -70,7 +70,7 @@ __device__ __forceinline__ void tile_tri(const DevMesh& m, const ClusterPlan& p,
                                          const typename tridev::Real<MIXED>::T (&c)[24], double area, double c2,
                                          double s2, double cs, typename tridev::Real<MIXED>::T (&f)[18]) {
     dev::TriMat<double> mt;
-    tridev::tri_hmu(m, t, mt.h, mt.mu);
+    tridev::tri_material(m, t, mt);
     mt.area = area;
     if (DIAL == DIAL_LCE) {
         double l2 = __dmul_rn(lam, lam), pp = pw;
@@ -96,7 +96,7 @@ __device__ __forceinline__ void tile_tri(const DevMesh& m, const ClusterPlan& p,
         P[sl][1] = __ldg(pos + m.N + ids[sl]);
         P[sl][2] = __ldg(pos + 2 * m.N + ids[sl]);
     }
-    tridev::tri_forces<MIXED>(P, c, mt, m.nu, m.gamma, f);
+    tridev::tri_forces<MIXED>(P, c, mt, m.nu, f);
 }
 
 // Walks this block's tiles (blockIdx.x, then every gridDim.x-th) of T

@@ -36,14 +36,25 @@ __device__ __forceinline__ void stage_contrib(typename Real<MIXED>::T* __restric
     }
 }
 
-// Thickness and shear modulus of triangle t.
-__device__ __forceinline__ void tri_hmu(const DevMesh& m, int t, double& h, double& mu) {
+// Material of one triangle with thickness h and shear modulus mu: h, mu and
+// their stretch / bend coefficients (the divisions of dev::material_coefs).
+__device__ __forceinline__ void set_material(double h, double mu, double nu, double gamma, TriMat<double>& mt) {
+    mt.h = h;
+    mt.mu = mu;
+    dev::material_coefs(h, mu, nu, gamma, mt.ks, mt.kb, mt.igmh);
+}
+
+// Material of triangle t: the uniform material's coefficients formed on the
+// host, or the triangle's own thickness and shear modulus.
+__device__ __forceinline__ void tri_material(const DevMesh& m, int t, TriMat<double>& mt) {
     if (m.uniform_hmu) {
-        h = m.h_uniform;
-        mu = m.mu_uniform;
+        mt.h = m.h_uniform;
+        mt.mu = m.mu_uniform;
+        mt.ks = m.ks_uniform;
+        mt.kb = m.kb_uniform;
+        mt.igmh = m.igmh_uniform;
     } else {
-        h = __ldg(m.thick + t);
-        mu = __ldg(m.shear + t);
+        set_material(__ldg(m.thick + t), __ldg(m.shear + t), m.nu, m.gamma, mt);
     }
 }
 
@@ -67,7 +78,7 @@ __device__ __forceinline__ void lce_metric(double c2, double s2, double cs, doub
 // tensors mt.
 template <bool MIXED>
 __device__ __forceinline__ void tri_forces(const double (&P)[6][3], const typename Real<MIXED>::T (&c)[24],
-                                           const TriMat<double>& mt, double nu, double gamma,
+                                           const TriMat<double>& mt, double nu,
                                            typename Real<MIXED>::T (&f)[18]) {
     using R = typename Real<MIXED>::T;
     Cq<R> q;
@@ -94,7 +105,7 @@ __device__ __forceinline__ void tri_forces(const double (&P)[6][3], const typena
         q.rxx = {rxx[0], rxx[1], rxx[2]};
         q.rxy = {rxy[0], rxy[1], rxy[2]};
         q.ryy = {ryy[0], ryy[1], ryy[2]};
-        dev::energy_gradient<double>(q, mt, nu, gamma, g);
+        dev::energy_gradient<double>(q, mt, nu, g);
     } else {
         // Positions relative to vertex 0, formed in double.  The first
         // derivatives and the metric a (hence the strain a - abar) are
@@ -137,10 +148,11 @@ __device__ __forceinline__ void tri_forces(const double (&P)[6][3], const typena
         q.rxy = {rxy[0], rxy[1], rxy[2]};
         q.ryy = {ryy[0], ryy[1], ryy[2]};
         double sp, bp;
-        dev::prefactors<double>(mt, nu, sp, bp);
+        dev::prefactors<double>(mt, sp, bp);
         const TriMat<float> mf = {(float)mt.abar0, (float)mt.abar1, (float)mt.abar2, (float)mt.bbar0,
-                                  (float)mt.bbar1, (float)mt.bbar2, (float)mt.h, (float)mt.mu, (float)mt.area};
-        dev::energy_gradient_strain<float>(q, mf, (float)nu, (float)gamma, (float)sp, (float)bp,
+                                  (float)mt.bbar1, (float)mt.bbar2, (float)mt.h,    (float)mt.mu,
+                                  (float)mt.area,  (float)mt.ks,    (float)mt.kb,    (float)mt.igmh};
+        dev::energy_gradient_strain<float>(q, mf, (float)nu, (float)sp, (float)bp,
                                            (float)(a0 - mt.abar0), (float)(a1 - mt.abar1), (float)(a2 - mt.abar2), g);
     }
 #pragma unroll
@@ -163,20 +175,17 @@ __device__ __forceinline__ void tri_forces(const double (&P)[6][3], const typena
 }
 
 
-// Contributions of triangle t read from the per-triangle (AoS) tables.
+// Contributions of triangle t read from the per-triangle (AoS) tables; mt
+// holds the triangle's material (h, mu and their coefficients).
 // With DIAL_LCE the programmed metric is protocol 3 at (dial, lam = lambda,
 // pw = lambda^(-2 nu_ot)) over the director trigonometry in p.tri_aux;
 // otherwise it is read from m.abar / m.bbar.
 template <int DIAL, bool MIXED>
 __device__ __forceinline__ void tri_contrib(const DevMesh& m, const ClusterPlan& p, const double* __restrict__ pos,
                                             int t, const int (&ids)[6], double dial, double lam, double pw,
-                                            typename Real<MIXED>::T (&f)[18], double nu, double gamma, double h,
-                                            double mu) {
+                                            typename Real<MIXED>::T (&f)[18], double nu, TriMat<double> mt) {
     using R = typename Real<MIXED>::T;
     const int N = m.N;
-    TriMat<double> mt;
-    mt.h = h;
-    mt.mu = mu;
     if (DIAL == DIAL_LCE) {
         const double2* ap = reinterpret_cast<const double2*>(p.tri_aux + t);
         const double2 a01 = __ldg(ap), a23 = __ldg(ap + 1);
@@ -225,7 +234,7 @@ __device__ __forceinline__ void tri_contrib(const DevMesh& m, const ClusterPlan&
         P[s][1] = __ldg(pos + N + ids[s]);
         P[s][2] = __ldg(pos + 2 * N + ids[s]);
     }
-    tri_forces<MIXED>(P, c, mt, nu, gamma, f);
+    tri_forces<MIXED>(P, c, mt, nu, f);
 }
 
 }  // namespace tridev

@@ -52,13 +52,29 @@ struct Cq {
     V3<R> rx, ry, rxx, rxy, ryy;
 };
 
-// Material and programmed-tensor inputs of one triangle.
+// Material and programmed-tensor inputs of one triangle.  ks, kb and igmh
+// are the material's stretch and bend coefficients and the bend-stiffening
+// scale (material_coefs), formed once per material rather than per triangle
+// so that the per-triangle chain carries no division.
 template <typename R>
 struct TriMat {
     R abar0, abar1, abar2;
     R bbar0, bbar1, bbar2;
     R h, mu, area;
+    R ks, kb, igmh;
 };
+
+// ks = 2 h mu / (1 - nu), kb = mu h^3 / (6 (1 - nu)), igmh = 1 / (gamma mu h).
+// Host and device evaluate the same expressions (products and correctly
+// rounded divisions only), so a constant formed on the host for a uniform
+// material has the bits the device forms per triangle otherwise.
+template <typename R>
+__host__ __device__ __forceinline__ void material_coefs(R h, R mu, R nu, R gamma, R& ks, R& kb, R& igmh) {
+    const R omn = R(1) - nu;
+    ks = R(2) * h * mu / omn;
+    kb = mu * h * h * h / (R(6) * omn);
+    igmh = R(1) / (gamma * mu * h);
+}
 
 // dE_t / d(cq), grouped as the 5 vector derivatives.
 template <typename R>
@@ -98,41 +114,41 @@ __device__ __forceinline__ R quad_form(R abar0, R abar1, R abar2, R d0, R d1, R 
 }
 
 // Stretch and bend prefactors sp, bp of one triangle (they hold the metric
-// inverse through det(abar)^(-3/2)).
+// inverse through det(abar)^(-3/2), formed as the cube of one reciprocal
+// square root: a few ulp, and no division on the chain).
 template <typename R>
-__device__ __forceinline__ void prefactors(const TriMat<R>& m, R nu, R& sp, R& bp) {
+__device__ __forceinline__ void prefactors(const TriMat<R>& m, R& sp, R& bp) {
     const R det = m.abar0 * m.abar2 - m.abar1 * m.abar1;
-    const R inv_det = R(1) / det;
-    const R det_m32 = inv_det * rsqrt_r(det);
-    const R omn = R(1) - nu;
-    sp = R(2) * m.h * m.mu * det_m32 / omn;
-    bp = m.mu * m.h * m.h * m.h * det_m32 / (R(6) * omn);
+    const R r = rsqrt_r(det);
+    const R det_m32 = r * r * r;
+    sp = m.ks * det_m32;
+    bp = m.kb * det_m32;
 }
 
 template <typename R>
-__device__ __forceinline__ void energy_gradient_pref(const Cq<R>& c, const TriMat<R>& m, R nu, R gamma, R sp, R bp,
+__device__ __forceinline__ void energy_gradient_pref(const Cq<R>& c, const TriMat<R>& m, R nu, R sp, R bp,
                                                      CqGrad<R>& g, R* w_stretch = nullptr, R* w_bend = nullptr);
 template <typename R>
-__device__ __forceinline__ void energy_gradient_strain(const Cq<R>& c, const TriMat<R>& m, R nu, R gamma, R sp, R bp,
-                                                       R d0, R d1, R d2, CqGrad<R>& g, R* w_stretch = nullptr,
+__device__ __forceinline__ void energy_gradient_strain(const Cq<R>& c, const TriMat<R>& m, R nu, R sp, R bp, R d0,
+                                                       R d1, R d2, CqGrad<R>& g, R* w_stretch = nullptr,
                                                        R* w_bend = nullptr);
 
 // Energy gradient of one triangle.  Also returns the stretch and bend
 // (stiffened) energy densities, used by the energy reductions.
 template <typename R>
-__device__ __forceinline__ void energy_gradient(const Cq<R>& c, const TriMat<R>& m, R nu, R gamma, CqGrad<R>& g,
+__device__ __forceinline__ void energy_gradient(const Cq<R>& c, const TriMat<R>& m, R nu, CqGrad<R>& g,
                                                 R* w_stretch = nullptr, R* w_bend = nullptr) {
     R sp, bp;
-    prefactors(m, nu, sp, bp);
-    energy_gradient_pref(c, m, nu, gamma, sp, bp, g, w_stretch, w_bend);
+    prefactors(m, sp, bp);
+    energy_gradient_pref(c, m, nu, sp, bp, g, w_stretch, w_bend);
 }
 
 // The same with the prefactors given.
 template <typename R>
-__device__ __forceinline__ void energy_gradient_pref(const Cq<R>& c, const TriMat<R>& m, R nu, R gamma, R sp, R bp,
+__device__ __forceinline__ void energy_gradient_pref(const Cq<R>& c, const TriMat<R>& m, R nu, R sp, R bp,
                                                      CqGrad<R>& g, R* w_stretch, R* w_bend) {
     const R a0 = dot(c.rx, c.rx), a1 = dot(c.rx, c.ry), a2 = dot(c.ry, c.ry);
-    energy_gradient_strain(c, m, nu, gamma, sp, bp, a0 - m.abar0, a1 - m.abar1, a2 - m.abar2, g, w_stretch, w_bend);
+    energy_gradient_strain(c, m, nu, sp, bp, a0 - m.abar0, a1 - m.abar1, a2 - m.abar2, g, w_stretch, w_bend);
 }
 
 // The same with the stretch strain d = a - abar given.  The mixed-precision
@@ -140,8 +156,8 @@ __device__ __forceinline__ void energy_gradient_pref(const Cq<R>& c, const TriMa
 // lose most of d's digits) and the prefactors in double, and runs the rest in
 // float.
 template <typename R>
-__device__ __forceinline__ void energy_gradient_strain(const Cq<R>& c, const TriMat<R>& m, R nu, R gamma, R sp, R bp,
-                                                       R d0, R d1, R d2, CqGrad<R>& g, R* w_stretch, R* w_bend) {
+__device__ __forceinline__ void energy_gradient_strain(const Cq<R>& c, const TriMat<R>& m, R nu, R sp, R bp, R d0,
+                                                       R d1, R d2, CqGrad<R>& g, R* w_stretch, R* w_bend) {
     // Stretch.
     R qs0, qs1, qs2;
     const R ws = quad_form(m.abar0, m.abar1, m.abar2, d0, d1, d2, nu, qs0, qs1, qs2);
@@ -156,7 +172,7 @@ __device__ __forceinline__ void energy_gradient_strain(const Cq<R>& c, const Tri
     R qb0, qb1, qb2;
     const R wb_raw = quad_form(m.abar0, m.abar1, m.abar2, b0 - m.bbar0, b1 - m.bbar1, b2 - m.bbar2, nu, qb0, qb1, qb2);
     const R wb = R(0.5) * bp * wb_raw;
-    const R fac = R(1) + R(2) * wb / (gamma * m.mu * m.h);
+    const R fac = R(1) + R(2) * wb * m.igmh;
     const R bpf = bp * fac;
     const R be0 = bpf * qb0, be1 = bpf * qb1, be2 = bpf * qb2;
 
@@ -182,7 +198,7 @@ __device__ __forceinline__ void energy_gradient_strain(const Cq<R>& c, const Tri
     g.rxy = {Ab1 * n.x, Ab1 * n.y, Ab1 * n.z};
     g.ryy = {Ab2 * n.x, Ab2 * n.y, Ab2 * n.z};
     if (w_stretch) *w_stretch = R(0.5) * sp * ws;
-    if (w_bend) *w_bend = wb * (R(1) + wb / (gamma * m.mu * m.h));
+    if (w_bend) *w_bend = wb * (R(1) + wb * m.igmh);
 }
 
 // LCE metric of dialling protocol 3 (do_dialling.cpp:112-123): lambda along

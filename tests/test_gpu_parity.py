@@ -127,7 +127,7 @@ def test_a_b_normals(workdir):
 
 
 def test_fused_step_matches_per_function_path(workdir):
-    """ms_step_n (two fused kernels per step) against the one-call-per-function
+    """ms_step_n (the fused step) against the one-call-per-function
     sequence on the same device: same state after 50 steps."""
     from morphoshell_b200 import GpuLoop
     m = make_model(workdir, "disk50")
