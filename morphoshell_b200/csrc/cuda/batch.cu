@@ -836,7 +836,7 @@ ms_status ms_batch_create(const ms_batch_instance* inst, int32_t n, int32_t devi
         int NT = 0, blocks = 0;
         auto smem_for = [&](const NodeTileLayout& lay, int nodes) { return node_tile_smem(lay.stride, nodes, mixed); };
         if (!choose_node_tiles(patch6.data(), (int)N, (int)T, mixed, sms, mixed ? MSB_NT_MINB_MIXED : MSB_NT_MINB,
-                               mixed ? 1008 : 928, 256, off, ent, smem_for, blocks_for, L, NT, blocks, err))
+                               mixed ? 1008 : 1100, 256, off, ent, smem_for, blocks_for, L, NT, blocks, err))
             return bail(bfail(b, MS_ERR_INVALID_ARGUMENT, err));
         if (blocks > 0) {
             std::vector<unsigned char> rec;

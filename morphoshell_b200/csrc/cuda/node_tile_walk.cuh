@@ -1,6 +1,6 @@
 // The chunk walk of the node-tiled step, shared by the single-mesh kernel
 // (node_tiles.cu) and the batched one (batch.cu).  A block takes node tiles
-// blockIdx.x, then every gridDim.x-th; for each tile it streams the chunk
+// blockIdx.x, then every gridDim.x-th; for each tile it walks the chunk
 // records of the tile's triangle list (NodeTilePlan), calls
 //   tri(t, ids, c, area, c2, s2, cs, f)
 // for every live triangle slot (t its triangle when need_t, else 0; f the 18
@@ -11,6 +11,15 @@
 // for each node of the tile with its summed deformation force.  A copy that
 // does not land within the bounded wait sets *err_flag to 5 (MS_ERR_TIMEOUT)
 // when it was 0 and ends the walk.
+//
+// A chunk record is its tables (ids, weights, trigonometry; field-major, so
+// slot i of every table is one coalesced warp load) followed by its node
+// section.  Each thread loads its slot's tables straight into registers,
+// for the next chunk while the block adds up the current one's runs, so the
+// loads are in flight across the runs and the barrier; only the node section
+// is bulk-copied into shared memory (two slots, one mbarrier).  Shared
+// memory per block is the contribution staging area, the two node-section
+// slots and the tile's accumulators, small enough for four blocks per SM.
 #pragma once
 
 #include <cstdint>
@@ -22,18 +31,62 @@
 namespace msb {
 namespace tiles {
 
-// Shared memory of a block: the chunk's fixed part (ids, weights,
-// trigonometry; single-buffered: it is refilled as soon as every thread holds
-// its triangle's tables in registers), the contribution staging area, two
-// node sections (the current chunk's, and the next one landing) and the
-// tile's per-node accumulators.
+// Shared memory of a block: the contribution staging area, two node
+// sections (the current chunk's, and the next one landing) and the tile's
+// per-node accumulators.  `fixed` is the tables' part of a record, read
+// straight into registers.
 template <bool MIXED>
 struct NtSmem {
     static constexpr size_t fixed = TileLayout<MIXED>::bytes;
     static constexpr size_t stage = (size_t)kTile * 18 * (MIXED ? 4 : 8);
     __host__ __device__ static size_t ns_cap(size_t stride) { return stride - fixed; }
     __host__ __device__ static size_t bytes(size_t stride, int nodes) {
-        return fixed + stage + 2 * ns_cap(stride) + 24 * (size_t)nodes;
+        return stage + 2 * ns_cap(stride) + 24 * (size_t)nodes;
+    }
+};
+
+// Streamed once per step: kept out of L1, where the position gathers live.
+__device__ __forceinline__ int ld_stream(const int* p) {
+    int v;
+    asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float ld_stream(const float* p) {
+    float v;
+    asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double ld_stream(const double* p) {
+    double v;
+    asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+
+// Slot i's tables of one chunk record, in registers.
+template <bool MIXED>
+struct SlotTables {
+    using R = typename tridev::Real<MIXED>::T;
+    int ids[6];
+    R cf[24];
+    double area, c2, s2, cs;
+    int t;
+
+    __device__ __forceinline__ void load(const unsigned char* __restrict__ rec, int i, int c, bool need_t,
+                                         const int* __restrict__ chunk_tri) {
+        using L = TileLayout<MIXED>;
+        const int* sid = reinterpret_cast<const int*>(rec);
+        const R* scoef = reinterpret_cast<const R*>(rec + L::ids);
+        const double* saux = reinterpret_cast<const double*>(rec + L::ids + L::coef);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) ids[k] = ld_stream(sid + k * kTile + i);
+#pragma unroll
+        for (int k = 0; k < 24; ++k) cf[k] = ld_stream(scoef + k * kTile + i);
+        area = ld_stream(saux + i);
+        c2 = ld_stream(saux + kTile + i);
+        s2 = ld_stream(saux + 2 * kTile + i);
+        cs = ld_stream(saux + 3 * kTile + i);
+        // Empty slots of a chunk hold -1 here; they are never computed.
+        t = need_t ? __ldg(chunk_tri + (size_t)c * kTile + i) : 0;
     }
 };
 
@@ -41,14 +94,12 @@ template <bool MIXED, typename Tri, typename Node>
 __device__ __forceinline__ void node_tile_walk(const NodeTilePlan& q, int N, bool need_t, int* err_flag, Tri tri,
                                                Node node) {
     using R = typename tridev::Real<MIXED>::T;
-    using L = TileLayout<MIXED>;
     using SM = NtSmem<MIXED>;
     extern __shared__ __align__(128) unsigned char nt_smem[];
     __shared__ uint64_t bar;
     const size_t ns_cap = SM::ns_cap(q.stride);
-    unsigned char* fx = nt_smem;
-    R* stage = reinterpret_cast<R*>(nt_smem + SM::fixed);
-    unsigned char* nsec = nt_smem + SM::fixed + SM::stage;
+    R* stage = reinterpret_cast<R*>(nt_smem);
+    unsigned char* nsec = nt_smem + SM::stage;
     double* acc = reinterpret_cast<double*>(nsec + 2 * ns_cap);
     const int i = threadIdx.x;
     for (int j = i; j < 3 * q.nodes; j += kTile) acc[j] = 0.0;
@@ -57,26 +108,17 @@ __device__ __forceinline__ void node_tile_walk(const NodeTilePlan& q, int N, boo
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
-    // Thread 0: chunk c's fixed part into the fixed area and its node section
-    // into node-section slot `slot`, both counted on the one barrier.
+    // Thread 0: chunk c's node section into node-section slot `slot`.
     auto fetch = [&](int c, int slot) {
-        const unsigned char* src = q.rec + (size_t)c * q.stride;
+        const unsigned char* src = q.rec + (size_t)c * q.stride + SM::fixed;
         const uint32_t nb = __ldg(q.chunk_bytes + c) - (uint32_t)SM::fixed;
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)),
-                     "r"((uint32_t)SM::fixed + nb)
-                     : "memory");
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                         smem_addr(fx)),
-                     "l"(src), "r"((uint32_t)SM::fixed), "r"(smem_addr(&bar))
-                     : "memory");
-        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                         smem_addr(nsec + slot * ns_cap)),
-                     "l"(src + SM::fixed), "r"(nb), "r"(smem_addr(&bar))
-                     : "memory");
+        bulk_load(nsec + slot * ns_cap, src, nb, &bar);
     };
     int tile = blockIdx.x;  // the grid is at most the tile count
     int c = __ldg(q.tile_chunk + tile);
     if (i == 0) fetch(c, 0);
+    SlotTables<MIXED> tb;
+    tb.load(q.rec + (size_t)c * q.stride, i, c, need_t, q.chunk_tri);
     uint32_t phase = 0u;
     int slot = 0;  // node-section slot of the current chunk
     for (;;) {
@@ -96,33 +138,18 @@ __device__ __forceinline__ void node_tile_walk(const NodeTilePlan& q, int N, boo
                 if (i == 0) atomicCAS(err_flag, 0, 5);  // MS_ERR_TIMEOUT
                 return;
             }
+            if (i == 0 && nc >= 0) fetch(nc, slot ^ 1);
             const unsigned char* ns = nsec + slot * ns_cap;
             const int4 hd = *reinterpret_cast<const int4*>(ns);  // R, E, ntri
-            const int* sid = reinterpret_cast<const int*>(fx);
-            const R* scoef = reinterpret_cast<const R*>(fx + L::ids);
-            const double* saux = reinterpret_cast<const double*>(fx + L::ids + L::coef);
-            int ids[6];
-            R cf[24];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) ids[k] = sid[k * kTile + i];
-#pragma unroll
-            for (int k = 0; k < 24; ++k) cf[k] = scoef[k * kTile + i];
-            const double area = saux[i], c2 = saux[kTile + i], s2 = saux[2 * kTile + i], cs = saux[3 * kTile + i];
-            const bool live = i < hd.z;
-            const int t = (need_t && live) ? __ldg(q.chunk_tri + (size_t)c * kTile + i) : 0;
-            // The table loads above may still be in flight (their values are
-            // used after the barrier): order them before the bulk copy that
-            // refills the area.
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
-            if (i == 0 && nc >= 0) fetch(nc, slot ^ 1);
             R f[18];
 #pragma unroll
             for (int j = 0; j < 18; ++j) f[j] = R(0);
-            if (live) tri(t, ids, cf, area, c2, s2, cs, f);
+            if (i < hd.z) tri(tb.t, tb.ids, tb.cf, tb.area, tb.c2, tb.s2, tb.cs, f);
 #pragma unroll
             for (int k = 0; k < 18; ++k) stage[k * kTile + i] = f[k];
             __syncthreads();
+            // The next chunk's tables load while this chunk's runs add up.
+            if (nc >= 0) tb.load(q.rec + (size_t)nc * q.stride, i, nc, need_t, q.chunk_tri);
             // Runs: one node's entries of this chunk each, distinct nodes, so
             // the runs of a chunk add in parallel without conflicts.  Staging
             // is field-major: component k of patch slot sl of the chunk's
@@ -146,14 +173,15 @@ __device__ __forceinline__ void node_tile_walk(const NodeTilePlan& q, int N, boo
                 acc[3 * j + 1] = a1;
                 acc[3 * j + 2] = a2;
             }
+            // The node-section reads above come before the bulk copy that
+            // refills this slot (issued after the next barrier).
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             slot ^= 1;
         }
         // The tile's nodes: every contribution is in once the runs of the
         // last chunk are done.  Each thread clears the accumulators it reads,
         // ready for the next tile (whose first runs come after at least two
-        // more block barriers).  One node at a time: loads of two in flight
-        // spill at the register budget of 3 blocks per SM and were measured
-        // slower.
+        // more block barriers).
         __syncthreads();
         for (int j = i; j < nn; j += kTile) {
             const double Fx = acc[3 * j], Fy = acc[3 * j + 1], Fz = acc[3 * j + 2];

@@ -2,22 +2,22 @@
 // with no per-triangle contributions in HBM.
 //
 // A persistent block walks node tiles (blockIdx.x, then every gridDim.x-th).
-// For each tile it streams the chunk records of the tile's triangle list
+// For each tile it walks the chunk records of the tile's triangle list
 // (every triangle whose patch touches one of the tile's nodes, ascending t).
-// Thread 0 copies a record with two cp.async.bulk (the tables into the
-// block's single table area, the node section into one of two slots;
-// completion counted in bytes on one mbarrier).  The copy of the next record
-// starts as soon as every thread holds its triangle's tables in registers,
-// so it lands while the block computes: each thread forms one triangle's 18
-// contributions (the arithmetic of the bulk-copy per-triangle kernel,
-// tile_tri) and stages them in a field-major area, and then the chunk's runs
-// add them to the tile's per-node accumulators in shared memory: one thread
-// per run, a run being one node's entries in this chunk in ascending
-// triangle order.  Chunks are taken in order, so each node's force is summed
-// in ascending triangle order from zero -- the order, and so the bits, of
-// the node kernel's gather (calc_deformation_forces.cpp:185).  After the
-// tile's last chunk the block finishes its nodes (damping, constraints,
-// guard, equilibrium maxima, symplectic Euler; node_core) and moves on.
+// Each thread reads its slot's tables (ids, weights, trigonometry) straight
+// into registers -- the next chunk's while the block adds up the current
+// one's runs -- and thread 0 bulk-copies the chunk's node section into one
+// of two shared-memory slots (completion counted in bytes on one mbarrier).
+// Each thread forms one triangle's 18 contributions (the arithmetic of the
+// bulk-copy per-triangle kernel, tile_tri) and stages them in a field-major
+// area, and then the chunk's runs add them to the tile's per-node
+// accumulators in shared memory: one thread per run, a run being one node's
+// entries in this chunk in ascending triangle order.  Chunks are taken in
+// order, so each node's force is summed in ascending triangle order from
+// zero -- the order, and so the bits, of the node kernel's gather
+// (calc_deformation_forces.cpp:185).  After the tile's last chunk the block
+// finishes its nodes (damping, constraints, guard, equilibrium maxima,
+// symplectic Euler; node_core) and moves on.
 //
 // Cost against the two-kernel step: triangles on tile borders are computed
 // once per tile they touch (about 20 % more triangle work at 700-node
@@ -40,7 +40,7 @@ using namespace tridev;
 using namespace tiles;
 
 // Resident blocks asked of the compiler (registers): FP64 at 3 per SM (168
-// registers), mixed at 4 (128).
+// registers; at 4 it spills and was measured slower), mixed at 4 (128).
 #ifndef MSB_NT_MINB
 #define MSB_NT_MINB 3
 #endif
