@@ -45,20 +45,28 @@ struct NtSmem {
     }
 };
 
-// Streamed once per step: kept out of L1, where the position gathers live.
-__device__ __forceinline__ int ld_stream(const int* p) {
+// The records stream once per step: their loads bypass L1 (where the
+// position gathers live) and carry an L2 evict-first policy, so that the
+// node state the previous step wrote stays in L2 for this step's gathers
+// (measured 2-3 % faster per step on the 1.8M-triangle disk).
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ int ld_stream(const int* p, uint64_t pol) {
     int v;
-    asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
     return v;
 }
-__device__ __forceinline__ float ld_stream(const float* p) {
+__device__ __forceinline__ float ld_stream(const float* p, uint64_t pol) {
     float v;
-    asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
     return v;
 }
-__device__ __forceinline__ double ld_stream(const double* p) {
+__device__ __forceinline__ double ld_stream(const double* p, uint64_t pol) {
     double v;
-    asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
     return v;
 }
 
@@ -72,19 +80,19 @@ struct SlotTables {
     int t;
 
     __device__ __forceinline__ void load(const unsigned char* __restrict__ rec, int i, int c, bool need_t,
-                                         const int* __restrict__ chunk_tri) {
+                                         const int* __restrict__ chunk_tri, uint64_t pol) {
         using L = TileLayout<MIXED>;
         const int* sid = reinterpret_cast<const int*>(rec);
         const R* scoef = reinterpret_cast<const R*>(rec + L::ids);
         const double* saux = reinterpret_cast<const double*>(rec + L::ids + L::coef);
 #pragma unroll
-        for (int k = 0; k < 6; ++k) ids[k] = ld_stream(sid + k * kTile + i);
+        for (int k = 0; k < 6; ++k) ids[k] = ld_stream(sid + k * kTile + i, pol);
 #pragma unroll
-        for (int k = 0; k < 24; ++k) cf[k] = ld_stream(scoef + k * kTile + i);
-        area = ld_stream(saux + i);
-        c2 = ld_stream(saux + kTile + i);
-        s2 = ld_stream(saux + 2 * kTile + i);
-        cs = ld_stream(saux + 3 * kTile + i);
+        for (int k = 0; k < 24; ++k) cf[k] = ld_stream(scoef + k * kTile + i, pol);
+        area = ld_stream(saux + i, pol);
+        c2 = ld_stream(saux + kTile + i, pol);
+        s2 = ld_stream(saux + 2 * kTile + i, pol);
+        cs = ld_stream(saux + 3 * kTile + i, pol);
         // Empty slots of a chunk hold -1 here; they are never computed.
         t = need_t ? __ldg(chunk_tri + (size_t)c * kTile + i) : 0;
     }
@@ -109,16 +117,23 @@ __device__ __forceinline__ void node_tile_walk(const NodeTilePlan& q, int N, boo
     }
     __syncthreads();
     // Thread 0: chunk c's node section into node-section slot `slot`.
+    const uint64_t pol = l2_evict_first_policy();
     auto fetch = [&](int c, int slot) {
         const unsigned char* src = q.rec + (size_t)c * q.stride + SM::fixed;
         const uint32_t nb = __ldg(q.chunk_bytes + c) - (uint32_t)SM::fixed;
-        bulk_load(nsec + slot * ns_cap, src, nb, &bar);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bar)), "r"(nb)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], "
+            "%4;" ::"r"(smem_addr(nsec + slot * ns_cap)),
+            "l"(src), "r"(nb), "r"(smem_addr(&bar)), "l"(pol)
+            : "memory");
     };
     int tile = blockIdx.x;  // the grid is at most the tile count
     int c = __ldg(q.tile_chunk + tile);
     if (i == 0) fetch(c, 0);
     SlotTables<MIXED> tb;
-    tb.load(q.rec + (size_t)c * q.stride, i, c, need_t, q.chunk_tri);
+    tb.load(q.rec + (size_t)c * q.stride, i, c, need_t, q.chunk_tri, pol);
     uint32_t phase = 0u;
     int slot = 0;  // node-section slot of the current chunk
     for (;;) {
@@ -149,7 +164,7 @@ __device__ __forceinline__ void node_tile_walk(const NodeTilePlan& q, int N, boo
             for (int k = 0; k < 18; ++k) stage[k * kTile + i] = f[k];
             __syncthreads();
             // The next chunk's tables load while this chunk's runs add up.
-            if (nc >= 0) tb.load(q.rec + (size_t)nc * q.stride, i, nc, need_t, q.chunk_tri);
+            if (nc >= 0) tb.load(q.rec + (size_t)nc * q.stride, i, nc, need_t, q.chunk_tri, pol);
             // Runs: one node's entries of this chunk each, distinct nodes, so
             // the runs of a chunk add in parallel without conflicts.  Staging
             // is field-major: component k of patch slot sl of the chunk's
