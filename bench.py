@@ -578,6 +578,7 @@ def ensemble_measurement(n: int, precision: str, warmup: int, steps: int, local:
     info = b.info()
     T = info["num_tris"]
     sched, tune_ms = b.autotune(steps_per_trial=8)
+    trials = b.autotune_report()
     b.run(warmup)
     stream = torch.cuda.ExternalStream(b.stream(), device=torch.device("cuda", local))
     e0 = torch.cuda.Event(enable_timing=True)
@@ -618,7 +619,8 @@ def ensemble_measurement(n: int, precision: str, warmup: int, steps: int, local:
                     "{+1, -1, +1/2}, h ~ U(0.005, 0.02), per-instance dialling state machines"
                     % (n, len(mine), min(sizes), max(sizes), T),
         "num_tris": T, "num_nodes": info["num_nodes"], "instances": n, "schedule": sched,
-        "autotune_ms_per_step": tune_ms, "host_setup_s": setup_s, "gpu_launches": per_step * done,
+        "autotune_ms_per_step": tune_ms, "autotune_trials": trials, "host_setup_s": setup_s,
+        "gpu_launches": per_step * done,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": peak_kind, "kernel": kernels + ", whole step",
                      "algorithmic_bytes_per_tri": bpt},
@@ -649,7 +651,8 @@ def run_ensemble(args):
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32/f64 mixed", "data": "synthetic",
         "config": {"workload": r["workload"], "precision": args.precision, "num_tris": r["num_tris"],
                    "num_nodes": r["num_nodes"], "instances": n, "schedule": r["schedule"],
-                   "autotune_ms_per_step": r["autotune_ms_per_step"], "host_setup_s": r["host_setup_s"],
+                   "autotune_ms_per_step": r["autotune_ms_per_step"], "autotune_trials": r["autotune_trials"],
+                   "host_setup_s": r["host_setup_s"],
                    "parallelism": "members split over %d GPUs" % world,
                    "l2": "inputs far larger than L2; no flush"},
         "gpu_launches": r["gpu_launches"],

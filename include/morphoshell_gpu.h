@@ -324,9 +324,13 @@ typedef struct ms_batch_inst_status {
  * persistent kernel fed by bulk-copied 128-triangle tiles; -1: the
  * node-tiled one-kernel step, node_block ignored -- the default when the
  * union has a node tile for every resident block, else 0) and of the
- * per-node kernel, steps per captured graph (even). */
+ * per-node kernel, steps per captured graph (even).  nodes_per_tile and
+ * blocks_per_sm describe the node-tiled plan in use (read by
+ * ms_batch_get_schedule, chosen by ms_batch_autotune; ignored by
+ * ms_batch_set_schedule). */
 typedef struct ms_batch_schedule {
     int32_t tri_block, node_block, chunk_steps;
+    int32_t nodes_per_tile, blocks_per_sm;
 } ms_batch_schedule;
 
 /* Only dialling protocol 3 without ansatz dialling and Newtonian dynamics
@@ -354,9 +358,15 @@ ms_status ms_batch_set_schedule(ms_batch* b, const ms_batch_schedule* s);
 ms_status ms_batch_get_schedule(const ms_batch* b, ms_batch_schedule* s);
 /* Times every built-in schedule on this batch (steps_per_trial steps each,
  * CUDA events) from the current state, puts the state back after each trial,
- * and keeps the fastest.  All schedules give the same bits. */
+ * and keeps the fastest; then rebuilds the node-tiled plan at other tile
+ * sizes and resident blocks per SM, times each the same way and keeps the
+ * fastest plan.  All schedules and plans give the same bits. */
 ms_status ms_batch_autotune(ms_batch* b, int32_t steps_per_trial, ms_batch_schedule* chosen,
                             double* best_ms_per_step);
+/* The last ms_batch_autotune's trials as text, one per line (schedule or
+ * node-tiled plan, ms per step): copies up to len - 1 bytes and a NUL into
+ * buf, returns the full length (-1 for a null batch). */
+int32_t ms_batch_autotune_report(const ms_batch* b, char* buf, int32_t len);
 ms_status ms_batch_info(const ms_batch* b, int64_t* num_nodes, int64_t* num_tris, int32_t* n_instances);
 void* ms_batch_stream(ms_batch* b);
 

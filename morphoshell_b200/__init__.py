@@ -30,7 +30,7 @@ GPU_SYMBOLS = [
     "ms_deformation_forces_noalloc", "ms_set_step_path", "ms_plan_info", "ms_node_tile_layout", "ms_node_tile_plan",
     "ms_batch_create", "ms_batch_destroy", "ms_batch_last_error", "ms_batch_run", "ms_batch_status",
     "ms_batch_download_dofs", "ms_batch_upload_dofs", "ms_batch_set_schedule", "ms_batch_get_schedule",
-    "ms_batch_autotune", "ms_batch_info", "ms_batch_stream", "ms_batch_set_start",
+    "ms_batch_autotune", "ms_batch_autotune_report", "ms_batch_info", "ms_batch_stream", "ms_batch_set_start",
     "ms_mlp_create", "ms_mlp_destroy", "ms_mlp_last_error", "ms_mlp_num_params", "ms_mlp_get_params",
     "ms_mlp_set_params", "ms_mlp_forward", "ms_mlp_loss_grad", "ms_mlp_set_data", "ms_mlp_train", "ms_mlp_stream",
 ]
@@ -121,7 +121,8 @@ class ms_batch_inst_status(C.Structure):
 
 
 class ms_batch_schedule(C.Structure):
-    _fields_ = [("tri_block", C.c_int32), ("node_block", C.c_int32), ("chunk_steps", C.c_int32)]
+    _fields_ = [("tri_block", C.c_int32), ("node_block", C.c_int32), ("chunk_steps", C.c_int32),
+                ("nodes_per_tile", C.c_int32), ("blocks_per_sm", C.c_int32)]
 
 
 MS_INST_DIALLING, MS_INST_WAITING, MS_INST_EQUIL, MS_INST_DONE, MS_INST_FAILED = range(5)
@@ -188,6 +189,8 @@ def lib() -> C.CDLL:
         L.ms_batch_set_start.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_int32]
         L.ms_batch_get_schedule.argtypes = [C.c_void_p, P(ms_batch_schedule)]
         L.ms_batch_autotune.argtypes = [C.c_void_p, C.c_int32, P(ms_batch_schedule), d]
+        L.ms_batch_autotune_report.argtypes = [C.c_void_p, C.c_char_p, C.c_int32]
+        L.ms_batch_autotune_report.restype = C.c_int32
         i64p = C.POINTER(C.c_int64)
         L.ms_batch_info.argtypes = [C.c_void_p, i64p, i64p, P(C.c_int32)]
         L.ms_batch_stream.argtypes = [C.c_void_p]
@@ -574,7 +577,7 @@ class Batch:
     def set_schedule(self, tri_block: int, node_block: int, chunk_steps: int):
         """tri_block -1: node-tiled one-kernel step (node_block ignored); 0:
         bulk-copy tile kernel; 64/128/256: per-triangle kernel block size."""
-        s = ms_batch_schedule(tri_block, node_block, chunk_steps)
+        s = ms_batch_schedule(tri_block, node_block, chunk_steps, 0, 0)
         self._chk(lib().ms_batch_set_schedule(self._h, C.byref(s)), "ms_batch_set_schedule")
 
     def autotune(self, steps_per_trial: int = 20):
@@ -582,6 +585,13 @@ class Batch:
         ms = np.zeros(1)
         self._chk(lib().ms_batch_autotune(self._h, steps_per_trial, C.byref(s), _dp(ms)), "ms_batch_autotune")
         return {k: getattr(s, k) for k, _ in s._fields_}, float(ms[0])
+
+    def autotune_report(self) -> list[str]:
+        """The last autotune's trials (schedule or node-tiled plan: ms per step)."""
+        n = lib().ms_batch_autotune_report(self._h, None, 0)
+        buf = C.create_string_buffer(max(n, 0) + 1)
+        lib().ms_batch_autotune_report(self._h, buf, len(buf))
+        return [ln for ln in buf.value.decode().splitlines() if ln]
 
     def info(self):
         N, T, n = C.c_int64(), C.c_int64(), C.c_int32()

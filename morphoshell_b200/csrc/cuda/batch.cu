@@ -257,6 +257,45 @@ __global__ void __launch_bounds__(kTile, MIXED ? MSB_NT_MINB_MIXED : MSB_NT_MINB
         });
 }
 
+// The tables part of the node-tiled records (ids, weights, area and
+// director trigonometry, field-major per chunk), gathered from the union's
+// per-triangle tables: the bytes fill_node_tile_records writes on the host.
+// One block per chunk, one thread per slot; empty slots get zeros.
+template <bool MIXED>
+__global__ void __launch_bounds__(kTile)
+    k_fill_node_tile_tables(unsigned char* __restrict__ rec, size_t stride, const int* __restrict__ chunk_tri,
+                            const int4* __restrict__ tri_idx, const typename Real<MIXED>::T* __restrict__ coef,
+                            const double4* __restrict__ aux) {
+    using R = typename Real<MIXED>::T;
+    using L = tiles::TileLayout<MIXED>;
+    const int c = blockIdx.x, i = threadIdx.x;
+    unsigned char* r = rec + (size_t)c * stride;
+    int* ids = reinterpret_cast<int*>(r);
+    R* cf = reinterpret_cast<R*>(r + L::ids);
+    double* ax = reinterpret_cast<double*>(r + L::ids + L::coef);
+    const int t = chunk_tri[(size_t)c * kTile + i];
+    if (t >= 0) {
+        const int4 a = tri_idx[2 * (size_t)t], b = tri_idx[2 * (size_t)t + 1];
+        const int id[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
+#pragma unroll
+        for (int k = 0; k < 6; ++k) ids[k * kTile + i] = id[k];
+#pragma unroll
+        for (int k = 0; k < 24; ++k) cf[k * kTile + i] = coef[24 * (size_t)t + k];
+        const double4 x = aux[t];
+        ax[i] = x.x;
+        ax[kTile + i] = x.y;
+        ax[2 * kTile + i] = x.z;
+        ax[3 * kTile + i] = x.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) ids[k * kTile + i] = 0;
+#pragma unroll
+        for (int k = 0; k < 24; ++k) cf[k * kTile + i] = R(0);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) ax[k * kTile + i] = 0.0;
+    }
+}
+
 constexpr int kPostBlock = 256;
 
 __global__ void __launch_bounds__(kPostBlock) k_batch_post(const InstParams* __restrict__ ip,
@@ -397,6 +436,9 @@ struct ms_batch {
     int tile_grid = 0;           // 0: tile kernel unavailable
     NodeTilePlan ntp{};          // node-tiled step over the union
     bool have_nt = false;
+    int nt_blocks = 0;           // resident blocks per SM the node-tiled plan runs at
+    std::string tune_report;     // the last autotune's trials, one per line
+    std::vector<void*> nt_allocs;  // the node-tiled plan's device buffers (replaced by the autotuner)
     int parity = 0;
     int sched = 0;
     int chunk = 64;
@@ -528,6 +570,80 @@ ms_status run_graph(ms_batch* b, int len, int parity, int sched) {
     b->graphs.push_back({len, parity, sched, exec});
     MB_CUDA(b, cudaGraphLaunch(exec, b->stream));
     return MS_OK;
+}
+
+// Device buffers of a node-tiled plan for a layout L of NT-node tiles run
+// at `blocks` resident blocks per SM: the node sections and slot triangles
+// from the host, the tables gathered on the device from the union's
+// per-triangle tables.  On success q describes the plan and allocs holds
+// its buffers (the caller frees them).
+ms_status plan_from_layout(ms_batch* b, const NodeTileLayout& L, int NT, int blocks, NodeTilePlan& q,
+                           std::vector<void*>& allocs) {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t pitch = L.stride - L.fixed;
+    std::vector<unsigned char> sections;
+    std::vector<int> ctri;
+    fill_node_sections(L, pitch, sections, ctri);
+    auto dal = [&](void** ptr, size_t bytes) -> ms_status {
+        cudaError_t e = cudaMalloc(ptr, std::max<size_t>(bytes, 1));
+        if (e != cudaSuccess) return bcuda(b, e, "cudaMalloc (node-tiled plan)");
+        allocs.push_back(*ptr);
+        return MS_OK;
+    };
+    unsigned char* d_rec;
+    int *d_tc, *d_ctri;
+    unsigned* d_bytes;
+    MB_TRY(dal(reinterpret_cast<void**>(&d_rec), L.stride * (size_t)L.C));
+    MB_TRY(dal(reinterpret_cast<void**>(&d_tc), sizeof(int) * L.tile_chunk.size()));
+    MB_TRY(dal(reinterpret_cast<void**>(&d_bytes), sizeof(unsigned) * L.bytes.size()));
+    MB_TRY(dal(reinterpret_cast<void**>(&d_ctri), sizeof(int) * ctri.size()));
+    MB_CUDA(b, cudaMemcpy(d_tc, L.tile_chunk.data(), sizeof(int) * L.tile_chunk.size(), cudaMemcpyHostToDevice));
+    MB_CUDA(b, cudaMemcpy(d_bytes, L.bytes.data(), sizeof(unsigned) * L.bytes.size(), cudaMemcpyHostToDevice));
+    MB_CUDA(b, cudaMemcpy(d_ctri, ctri.data(), sizeof(int) * ctri.size(), cudaMemcpyHostToDevice));
+    MB_CUDA(b, cudaMemcpy2D(d_rec + L.fixed, L.stride, sections.data(), pitch, pitch, (size_t)L.C,
+                            cudaMemcpyHostToDevice));
+    if (L.C > 0) {
+        if (b->precision == MS_PRECISION_MIXED)
+            k_fill_node_tile_tables<true><<<L.C, kTile, 0, b->stream>>>(d_rec, L.stride, d_ctri, b->p.tri_idx,
+                                                                        b->p.coef_aos_f, b->p.tri_aux);
+        else
+            k_fill_node_tile_tables<false><<<L.C, kTile, 0, b->stream>>>(d_rec, L.stride, d_ctri, b->p.tri_idx,
+                                                                         b->p.coef_aos, b->p.tri_aux);
+        MB_CUDA(b, cudaGetLastError());
+        MB_CUDA(b, cudaStreamSynchronize(b->stream));
+    }
+    q = NodeTilePlan{};
+    q.nodes = NT;
+    q.ntiles = L.K;
+    q.nchunks = L.C;
+    q.grid = sms * blocks;
+    q.stride = L.stride;
+    q.slc = L.slc_max;
+    q.rec = d_rec;
+    q.tile_chunk = d_tc;
+    q.chunk_bytes = d_bytes;
+    q.chunk_tri = d_ctri;
+    return MS_OK;
+}
+
+// Resident blocks per SM of the batched node-tiled kernel at `smem` bytes of
+// shared memory per block (0: it cannot run).
+int batch_node_tile_blocks(int mixed, size_t smem) {
+    int nb = 0;
+    cudaError_t ea = mixed ? cudaFuncSetAttribute(k_batch_node_tiles<true>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                           : cudaFuncSetAttribute(k_batch_node_tiles<false>,
+                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (ea == cudaSuccess)
+        ea = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batch_node_tiles<true>, kTile, smem)
+                   : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_batch_node_tiles<false>, kTile, smem);
+    if (ea != cudaSuccess) {
+        cudaGetLastError();
+        nb = 0;
+    }
+    return nb;
 }
 
 bool all_frozen(const ms_batch* b) {
@@ -815,22 +931,7 @@ ms_status ms_batch_create(const ms_batch_instance* inst, int32_t n, int32_t devi
         int dev = 0, sms = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        auto blocks_for = [&](size_t smem) {
-            int nb_ = 0;
-            cudaError_t ea = mixed ? cudaFuncSetAttribute(k_batch_node_tiles<true>,
-                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-                                   : cudaFuncSetAttribute(k_batch_node_tiles<false>,
-                                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (ea == cudaSuccess)
-                ea = mixed ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_, k_batch_node_tiles<true>, kTile, smem)
-                           : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_, k_batch_node_tiles<false>, kTile,
-                                                                           smem);
-            if (ea != cudaSuccess) {
-                cudaGetLastError();
-                nb_ = 0;
-            }
-            return nb_;
-        };
+        auto blocks_for = [&](size_t smem) { return batch_node_tile_blocks(mixed, smem); };
         NodeTileLayout L;
         std::string err;
         int NT = 0, blocks = 0;
@@ -839,27 +940,8 @@ ms_status ms_batch_create(const ms_batch_instance* inst, int32_t n, int32_t devi
                                mixed ? 1008 : 1100, 256, off, ent, smem_for, blocks_for, L, NT, blocks, err))
             return bail(bfail(b, MS_ERR_INVALID_ARGUMENT, err));
         if (blocks > 0) {
-            std::vector<unsigned char> rec;
-            std::vector<int> ctri;
-            fill_node_tile_records(L, patch6.data(), mixed ? nullptr : coef.data(), mixed ? mcoef.data() : nullptr,
-                                   nullptr, aux.data(), mixed, rec, ctri);
-            unsigned char* d_rec;
-            int *d_tc, *d_ctri;
-            unsigned* d_bytes;
-            if ((st = bupload(b, &d_rec, rec)) || (st = bupload(b, &d_tc, L.tile_chunk)) ||
-                (st = bupload(b, &d_bytes, L.bytes)) || (st = bupload(b, &d_ctri, ctri)))
-                return bail(st);
-            NodeTilePlan& q = b->ntp;
-            q.nodes = NT;
-            q.ntiles = L.K;
-            q.nchunks = L.C;
-            q.grid = sms * blocks;
-            q.stride = L.stride;
-            q.slc = L.slc_max;
-            q.rec = d_rec;
-            q.tile_chunk = d_tc;
-            q.chunk_bytes = d_bytes;
-            q.chunk_tri = d_ctri;
+            if ((st = plan_from_layout(b, L, NT, blocks, b->ntp, b->nt_allocs))) return bail(st);
+            b->nt_blocks = blocks;
             b->have_nt = true;
         }
         // The one-kernel step once every block has a tile of its own
@@ -898,6 +980,7 @@ void ms_batch_destroy(ms_batch* b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     clear_graphs(b);
     for (void* q : b->allocs) cudaFree(q);
+    for (void* q : b->nt_allocs) cudaFree(q);
     if (b->h_is) cudaFreeHost(b->h_is);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -1024,6 +1107,8 @@ ms_status ms_batch_get_schedule(const ms_batch* b, ms_batch_schedule* s) {
     s->tri_block = kScheds[b->sched].tri_block;
     s->node_block = kScheds[b->sched].node_block;
     s->chunk_steps = b->chunk;
+    s->nodes_per_tile = b->have_nt ? b->ntp.nodes : 0;
+    s->blocks_per_sm = b->have_nt ? b->nt_blocks : 0;
     return MS_OK;
 }
 
@@ -1071,10 +1156,14 @@ ms_status ms_batch_autotune(ms_batch* b, int32_t steps, ms_batch_schedule* chose
         return cudaMemcpyAsync(b->d_is, save_is, n * sizeof(InstState), cudaMemcpyDeviceToDevice, st);
     };
     if (copy_state(true) != cudaSuccess) rc = bcuda(b, cudaGetLastError(), "autotune save");
-    for (int k = 0; k < kNumScheds && rc == MS_OK; ++k) {
-        if (kScheds[k].tri_block == 0 && b->tile_grid == 0) continue;
-        if (kScheds[k].tri_block < 0 && !b->have_nt) continue;
-        // one untimed pass (graph instantiation, caches), then the timed one
+    const int mixed = b->precision == MS_PRECISION_MIXED;
+    std::string report;
+    // ms per step of schedule k from the saved state: one untimed pass
+    // (graph instantiation, caches), then the timed one; < 0 on error (rc).
+    auto time_sched = [&](int k) -> double {
+        if (kScheds[k].tri_block < 0)  // the launch's shared memory is the current plan's
+            batch_node_tile_blocks(mixed, node_tile_smem(b->ntp.stride, b->ntp.nodes, mixed));
+        double t = -1.0;
         for (int rep = 0; rep < 2 && rc == MS_OK; ++rep) {
             if (copy_state(false) != cudaSuccess) {
                 rc = bcuda(b, cudaGetLastError(), "autotune restore");
@@ -1090,11 +1179,90 @@ ms_status ms_batch_autotune(ms_batch* b, int32_t steps, ms_batch_schedule* chose
             }
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ev0, ev1);
-            if (rep == 1 && ms / steps < best) {
-                best = ms / steps;
-                best_k = k;
+            if (rep == 1) t = ms / steps;
+        }
+        return t;
+    };
+    double nt_ms = -1.0;
+    for (int k = 0; k < kNumScheds && rc == MS_OK; ++k) {
+        if (kScheds[k].tri_block == 0 && b->tile_grid == 0) continue;
+        if (kScheds[k].tri_block < 0 && !b->have_nt) continue;
+        const double t = time_sched(k);
+        if (t < 0) break;
+        char line[160];
+        std::snprintf(line, sizeof line, "schedule tri_block %d node_block %d%s: %.4f ms/step\n",
+                      kScheds[k].tri_block, kScheds[k].node_block,
+                      k == kSchedNodeTiles ? (" (" + std::to_string(b->ntp.nodes) + "-node tiles, " +
+                                              std::to_string(b->nt_blocks) + " blocks/SM)").c_str()
+                                           : "",
+                      t);
+        report += line;
+        if (k == kSchedNodeTiles) nt_ms = t;
+        if (t < best) {
+            best = t;
+            best_k = k;
+        }
+    }
+    // Tile size and resident blocks per SM of the node-tiled plan: rebuild
+    // it at smaller and larger tiles, and at larger tiles with one block per
+    // SM fewer, time each, keep the fastest (the plans give the same bits).
+    if (rc == MS_OK && nt_ms > 0) {
+        const int N = b->m.N, T = b->m.T;
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        std::vector<int4> idx(2ULL * T);
+        std::vector<int> patch6(6ULL * T), off(N + 1), ent(6ULL * T);
+        if (cudaMemcpy(idx.data(), b->p.tri_idx, sizeof(int4) * idx.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(off.data(), b->m.inc_off, sizeof(int) * off.size(), cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(ent.data(), b->m.inc_ent, sizeof(int) * ent.size(), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = bcuda(b, cudaGetLastError(), "autotune: incidence download");
+        for (long long t = 0; t < T && rc == MS_OK; ++t) {
+            const int4 a = idx[2 * t], c = idx[2 * t + 1];
+            const int id[6] = {a.x, a.y, a.z, a.w, c.x, c.y};
+            for (int k = 0; k < 6; ++k) patch6[6 * t + k] = id[k];
+        }
+        const int nt0 = b->ntp.nodes, b0 = b->nt_blocks;
+        const int cand[3][2] = {{nt0 * 7 / 10, b0}, {nt0 * 14 / 10, b0}, {nt0 * 2, b0 - 1}};
+        for (const auto& cd : cand) {
+            if (rc != MS_OK) break;
+            const int nt = std::max(256, std::min(cd[0], kNtMaxNodes)), nb = cd[1];
+            if (nb < 1 || nt == b->ntp.nodes) continue;
+            NodeTileLayout L;
+            std::string err;
+            if (!node_tile_layout(patch6.data(), N, T, nt, mixed, off, ent, L, err)) continue;
+            if (L.K < sms * nb || batch_node_tile_blocks(mixed, node_tile_smem(L.stride, nt, mixed)) < nb) continue;
+            NodeTilePlan q;
+            std::vector<void*> al;
+            const ms_status s2 = plan_from_layout(b, L, nt, nb, q, al);
+            if (s2 != MS_OK) {  // no room for a second plan: keep the current one
+                for (void* x : al) cudaFree(x);
+                cudaGetLastError();
+                if (s2 != MS_ERR_OUT_OF_MEMORY) rc = s2;
+                continue;
+            }
+            std::swap(b->ntp, q);
+            clear_graphs(b);
+            const double t = time_sched(kSchedNodeTiles);
+            char line[160];
+            std::snprintf(line, sizeof line, "node-tiled plan %d-node tiles, %d blocks/SM: %.4f ms/step\n", nt, nb, t);
+            report += line;
+            if (t > 0 && t < nt_ms) {
+                for (void* x : b->nt_allocs) cudaFree(x);
+                b->nt_allocs.swap(al);
+                b->nt_blocks = nb;
+                nt_ms = t;
+                if (t < best) {
+                    best = t;
+                    best_k = kSchedNodeTiles;
+                }
+            } else {
+                std::swap(b->ntp, q);
+                clear_graphs(b);
+                for (void* x : al) cudaFree(x);
             }
         }
+        batch_node_tile_blocks(mixed, node_tile_smem(b->ntp.stride, b->ntp.nodes, mixed));
     }
     if (copy_state(false) != cudaSuccess && rc == MS_OK) rc = bcuda(b, cudaGetLastError(), "autotune restore");
     cudaStreamSynchronize(st);
@@ -1108,9 +1276,21 @@ ms_status ms_batch_autotune(ms_batch* b, int32_t steps, ms_batch_schedule* chose
         return rc;
     }
     b->sched = best_k;
+    b->tune_report = report;
     if (chosen) ms_batch_get_schedule(b, chosen);
     if (best_ms) *best_ms = best;
     return MS_OK;
+}
+
+int32_t ms_batch_autotune_report(const ms_batch* b, char* buf, int32_t len) {
+    if (!b) return -1;
+    const int32_t n = (int32_t)b->tune_report.size();
+    if (buf && len > 0) {
+        const int32_t k = std::min(n, len - 1);
+        std::memcpy(buf, b->tune_report.data(), (size_t)k);
+        buf[k] = 0;
+    }
+    return n;
 }
 
 ms_status ms_batch_info(const ms_batch* b, int64_t* num_nodes, int64_t* num_tris, int32_t* n_instances) {

@@ -219,6 +219,12 @@ bool choose_node_tiles(const int* patch_ids, int N, int T, int mixed, int sms, i
 void fill_node_tile_records(const NodeTileLayout& L, const int* patch_ids, const double* coef_d, const float* coef_f,
                             const double* area, const double* aux4, int mixed, std::vector<unsigned char>& buf,
                             std::vector<int>& chunk_tri);
+// Only the node sections (chunk c's at sections[pitch c], pitch at least
+// the record's node-section room) and the triangle of every slot: the
+// tables part of the records is then gathered on the device
+// (batch.cu: fill_tables_on_device).
+void fill_node_sections(const NodeTileLayout& L, size_t pitch, std::vector<unsigned char>& sections,
+                        std::vector<int>& chunk_tri);
 
 // Layout of the per-(triangle, slot) force contributions: x, y, z doubles;
 // for the mixed path x, y, z floats, optionally padded with a zero to 16

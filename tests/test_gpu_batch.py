@@ -108,6 +108,31 @@ def test_batch_schedules_agree_and_autotune_keeps_state(tmp_path):
         assert np.array_equal(a.download(i)[0], b.download(i)[0])
 
 
+def test_autotune_searches_node_tile_plans_with_the_same_bits(tmp_path):
+    """On a union big enough for several tile sizes, the autotuner rebuilds
+    the node-tiled plan (tables gathered on the device) and times each; the
+    steps after it give the bits of the default plan."""
+    from morphoshell_b200 import Batch
+    models, _ = _members(tmp_path, [3, 5], spacing_range=(0.004, 0.0041))
+    a = Batch(models)
+    a.run(64)
+    sched, ms = a.autotune(steps_per_trial=8)
+    assert ms > 0 and sched["nodes_per_tile"] >= 256 and sched["blocks_per_sm"] >= 1, sched
+    trials = a.autotune_report()
+    assert sum("node-tiled plan" in t for t in trials) >= 1, trials
+    for i in range(2):
+        assert a.status(i).stepcount == 64
+    a.run(128)
+    b = Batch(models)
+    b.set_schedule(-1, 0, 64)
+    assert b.schedule()["nodes_per_tile"] >= 256
+    b.run(192)
+    for i in range(2):
+        xa, va = a.download(i)
+        xb, vb = b.download(i)
+        assert np.array_equal(xa, xb) and np.array_equal(va, vb)
+
+
 def test_batch_done_instance_freezes(tmp_path):
     """An instance that reaches equilibrium at dial factor 1 stops; its
     final state stays available while the run goes on for the rest."""
