@@ -45,7 +45,10 @@ typedef struct msh_scalars {
 } msh_scalars;
 
 /* settings_path and vtk_path as the reference's command line; ansatz_path
- * may be NULL.  flags: bit 0 quiet (no stdout), bit 1 skip the initial noise. */
+ * may be NULL.  flags: bit 0 quiet (no stdout), bit 1 skip the initial noise,
+ * bit 2 patch search, patch fit and derivative weights on the current CUDA
+ * device (the host's results, bit for bit; triangles whose candidate
+ * distances tie are redone on the host). */
 int msh_load(const char* settings_path, const char* vtk_path, const char* ansatz_path, int flags, msh_model** out);
 /* Same set-up with the mesh handed over in memory instead of a VTK file
  * (the CELL_DATA / POINT_DATA fields of read_vtk_data.cpp as arrays):

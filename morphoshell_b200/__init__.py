@@ -242,11 +242,13 @@ class Model:
     """Host set-up of one run (msh_load): settings + mesh (+ ansatz)."""
 
     def __init__(self, settings_path: str, vtk_path: str | None, ansatz_path: str | None = None,
-                 quiet: bool = True, noise: bool = True, _handle=None):
+                 quiet: bool = True, noise: bool = True, device_setup: bool = False, _handle=None):
+        """device_setup: patch search, patch fit and derivative weights on the
+        current CUDA device (the host set-up's results, bit for bit)."""
         L = lib()
         if _handle is None:
             h = C.c_void_p()
-            flags = (1 if quiet else 0) | (0 if noise else 2)
+            flags = (1 if quiet else 0) | (0 if noise else 2) | (4 if device_setup else 0)
             rc = L.msh_load(settings_path.encode(), vtk_path.encode(),
                             ansatz_path.encode() if ansatz_path else None, flags, C.byref(h))
             if rc != 0:
@@ -263,8 +265,10 @@ class Model:
 
     @classmethod
     def from_arrays(cls, settings_path: str, positions, tris, abar_info, bbar_info, thickness=None,
-                    shear_modulus=None, constrained=None, quiet: bool = True, noise: bool = True) -> "Model":
-        """Set-up from in-memory mesh arrays (msh_build) instead of a VTK file."""
+                    shear_modulus=None, constrained=None, quiet: bool = True, noise: bool = True,
+                    device_setup: bool = False) -> "Model":
+        """Set-up from in-memory mesh arrays (msh_build) instead of a VTK file;
+        device_setup as for the constructor."""
         L = lib()
         pos = np.ascontiguousarray(positions, dtype=np.float64)
         if pos.shape[1] == 2:
@@ -276,7 +280,7 @@ class Model:
         sm = None if shear_modulus is None else np.ascontiguousarray(shear_modulus, dtype=np.float64)
         cn = None if constrained is None else np.ascontiguousarray(constrained, dtype=np.uint8)
         h = C.c_void_p()
-        flags = (1 if quiet else 0) | (0 if noise else 2)
+        flags = (1 if quiet else 0) | (0 if noise else 2) | (4 if device_setup else 0)
         rc = L.msh_build(settings_path.encode(), pos.shape[0], tri.shape[0], _dp(pos),
                          tri.ctypes.data_as(C.POINTER(C.c_int32)), _dp(a), a.shape[1], _dp(b), b.shape[1], _dp(th),
                          _dp(sm), None if cn is None else cn.ctypes.data_as(C.POINTER(C.c_uint8)), flags, C.byref(h))

@@ -35,9 +35,13 @@ NVCCFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xco
 HOST_SOURCES = ["host/settings.cpp", "host/vtk_io.cpp", "host/mesh_setup.cpp", "host/host_capi.cpp"]
 CUDA_SOURCES = ["cuda/kernels.cu", "cuda/cluster.cu", "cuda/capi.cu", "cuda/noalloc.cu", "cuda/batch.cu",
                 "cuda/learned.cu", "cuda/tri_tiles.cu", "cuda/node_tiles.cu", "cuda/node_tile_plan.cu",
-                "cuda/node_pipe.cu"]
+                "cuda/node_pipe.cu", "cuda/setup.cu"]
+# Per-file nvcc flags: the device set-up rounds every operation as the host
+# set-up does (no contraction into fused multiply-adds).
+CUDA_FILE_FLAGS = {"cuda/setup.cu": ["-fmad=false"]}
 HEADERS = ["host/host.hpp", "host/small_linalg.hpp", "cuda/internal.cuh", "cuda/tri_physics.cuh", "cuda/step_common.cuh",
            "cuda/tri_contrib.cuh", "cuda/tc_gemm.cuh", "cuda/tile_copy.cuh", "cuda/node_tile_walk.cuh",
+           "host/patch_fit.hpp",
            "../../include/morphoshell_gpu.h", "../../include/morphoshell_host.h"]
 
 
@@ -73,7 +77,7 @@ def _compile(src_rel: str, force: bool, extra: list[str]) -> str:
 def build(force: bool = False, verbose_ptxas: bool = False) -> str:
     os.makedirs(OBJ_DIR, exist_ok=True)
     extra_cu = ["-Xptxas", "-v"] if verbose_ptxas else []
-    jobs = [(s, []) for s in HOST_SOURCES] + [(s, extra_cu) for s in CUDA_SOURCES]
+    jobs = [(s, []) for s in HOST_SOURCES] + [(s, extra_cu + CUDA_FILE_FLAGS.get(s, [])) for s in CUDA_SOURCES]
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 2)) as ex:
         objs = list(ex.map(lambda j: _compile(j[0], force, j[1]), jobs))
     if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):

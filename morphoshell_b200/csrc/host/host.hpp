@@ -162,6 +162,20 @@ void set_up_patch_fitting(const std::vector<Node>& nodes, const DMat& node_posit
 // the (xx, xy, yy) second-derivative weights].
 void calc_deriv_coeffs(std::vector<double>& coeffs, const DMat& node_positions,
                        const std::vector<Tri>& triangles, const Stuff& stuff);
+// One triangle's patch search and fit (the loop body of set_up_patch_fitting;
+// throws as it does), its 24 weights (calc_deriv_coeffs for one triangle) and
+// the set-up's retry report.
+void fit_patch(int t_index, const std::vector<Node>& nodes, const DMat& node_positions, std::vector<Tri>& triangles,
+               double thresh, int& num_interior_retries);
+void deriv_coeffs_of(const Tri& tri, const DMat& node_positions, double* coeffs24);
+void log_patch_retries(Log& log, int num_interior_retries);
+// set_up_patch_fitting and calc_deriv_coeffs on the current CUDA device
+// (setup.cu), with the same results: triangles whose candidate distances tie
+// (where the order std::sort gives them is the host's to decide) or whose
+// search the device cannot finish are redone on the host.
+void set_up_patches_on_device(const std::vector<Node>& nodes, const DMat& node_positions,
+                              std::vector<Tri>& triangles, const Stuff& stuff, std::vector<double>& coeffs,
+                              Log& log);
 void calc_dof_masses(std::vector<double>& dof_masses, const std::vector<Tri>& triangles,  // calc_dof_masses.cpp:45
                      const Stuff& stuff);
 void calc_char_mechanics_scales(const std::vector<Tri>& triangles, Stuff& stuff);         // calc_char_mechanics_scales.cpp:45

@@ -128,8 +128,12 @@ int load_common(const char* settings_path, const char* vtk_path, const ArrayMesh
         }
         if (st.dialling_from_ansatz_rather_than_ref_state) m->dial_factor_to_start_from = 0.0;
         calc_mesh_info(m->nodes, m->ref_positions, m->tris, m->edges, st, log);
-        set_up_patch_fitting(m->nodes, m->ref_positions, m->tris, st, log);
-        calc_deriv_coeffs(m->coeffs, m->ref_positions, m->tris, st);
+        if (flags & 4) {
+            set_up_patches_on_device(m->nodes, m->ref_positions, m->tris, st, m->coeffs, log);
+        } else {
+            set_up_patch_fitting(m->nodes, m->ref_positions, m->tris, st, log);
+            calc_deriv_coeffs(m->coeffs, m->ref_positions, m->tris, st);
+        }
         calc_dof_masses(m->mass, m->tris, st);
         calc_char_mechanics_scales(m->tris, st);
         calc_long_timescales(st, log);

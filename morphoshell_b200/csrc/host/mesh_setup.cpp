@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "host.hpp"
+#include "patch_fit.hpp"
 #include "small_linalg.hpp"
 
 namespace msb {
@@ -234,11 +235,74 @@ void parallel_ranges(int n, int threads, F f) {
 
 }  // namespace
 
+void log_patch_retries(Log& log, int num_interior_retries) {
+    log << "\nNumber of non-boundary triangles that had to search through \n"
+        << "multiple possible patch options to find one \nsatisfying the condition number "
+        << "criterion was " << num_interior_retries << ", \nwhich should not be a large proportion of the mesh's "
+        << "triangles." << std::endl;
+}
+
 // source_files/set_up_patch_fitting.cpp:48-305.  For each triangle, the
 // three extra patch nodes are the nearest candidates (vertices of triangles
 // incident on its vertices, nearest first) whose 6x6 quadratic-fit matrix is
 // invertible and well conditioned; the kept 6x3 block maps the six patch
 // nodes' values to the second derivatives (xx, xy, yy) at the centroid.
+void fit_patch(int t_index, const std::vector<Node>& nodes, const DMat& P, std::vector<Tri>& triangles,
+               double thresh, int& num_interior_retries) {
+    Tri& tri = triangles[t_index];
+    std::vector<double> dists;
+    std::vector<int> cands;
+    for (int v = 0; v < 3; ++v)
+        for (int it : nodes[tri.vertex_ids[v]].incident_tri_ids)
+            for (int w = 0; w < 3; ++w) {
+                int id = triangles[it].vertex_ids[w];
+                bool seen = (id == tri.vertex_ids[0] || id == tri.vertex_ids[1] || id == tri.vertex_ids[2]);
+                for (int c : cands) seen = seen || (c == id);
+                if (!seen) {
+                    dists.push_back(patch::centroid_distance(&P.v[static_cast<size_t>(id) * 3], tri.ref_centroid));
+                    cands.push_back(id);
+                }
+            }
+    if (cands.size() < 3)
+        throw std::runtime_error("At least one search for patch nodes was exhausted without success (triangle " +
+                                 std::to_string(tri.id) + "): fewer than 3 candidate patch nodes.");
+    std::vector<size_t> order(dists.size());
+    for (size_t q = 0; q < order.size(); ++q) order[q] = q;
+    std::sort(order.begin(), order.end(), [&dists](const size_t& a, const size_t& b) { return dists[a] < dists[b]; });
+    tri.non_vertex_patch_nodes_ids[0] = cands[order[0]];
+    bool success = false;
+    for (size_t p = 1; p < std::min<size_t>(4, order.size()) && !success; ++p) {
+        tri.non_vertex_patch_nodes_ids[1] = cands[order[p]];
+        for (size_t q = 2; q < cands.size(); ++q) {
+            tri.non_vertex_patch_nodes_ids[2] = cands[order[q]];
+            const int ids[6] = {tri.vertex_ids[0], tri.vertex_ids[1], tri.vertex_ids[2],
+                                tri.non_vertex_patch_nodes_ids[0], tri.non_vertex_patch_nodes_ids[1],
+                                tri.non_vertex_patch_nodes_ids[2]};
+            double pos[6][3];
+            for (int n = 0; n < 6; ++n)
+                for (int c = 0; c < 3; ++c) pos[n][c] = P(ids[n], c);
+            double block[6][3];
+            const bool accepted = patch::try_patch(pos, tri.ref_centroid, thresh, block);
+            if (!accepted) {
+                if (q == 2 && !tri.is_boundary) num_interior_retries += 1;
+                continue;
+            }
+            for (int r = 0; r < 6; ++r)
+                for (int c = 0; c < 3; ++c) tri.mat_for_patch_2nd_derivs[r][c] = block[r][c];
+            success = true;
+            break;
+        }
+    }
+    if (!success)
+        throw std::runtime_error(
+            "At least one search for patch nodes was exhausted without success (triangle " +
+            std::to_string(tri.id) +
+            "); all possible patch matrices in the search had a  condition number above the acceptance "
+            "threshold. Try increasing this threshold. If that does not solve the issue, or causes other "
+            "issues, either the patch node search will need to be extended, or you will need to use a nicer "
+            "mesh. Aborting.");
+}
+
 void set_up_patch_fitting(const std::vector<Node>& nodes, const DMat& P, std::vector<Tri>& triangles,
                           const Stuff& stuff, Log& log) {
     // Triangles are independent: ranges of them in parallel threads, each
@@ -246,94 +310,21 @@ void set_up_patch_fitting(const std::vector<Node>& nodes, const DMat& P, std::ve
     const int nt = setup_threads((int)triangles.size());
     std::vector<int> retries(nt, 0);
     parallel_ranges((int)triangles.size(), nt, [&](int t_begin, int t_end, int worker) {
-    int& num_interior_retries = retries[worker];
-    for (int t_index = t_begin; t_index < t_end; ++t_index) {
-        Tri& tri = triangles[t_index];
-        std::vector<double> dists;
-        std::vector<int> cands;
-        for (int v = 0; v < 3; ++v)
-            for (int it : nodes[tri.vertex_ids[v]].incident_tri_ids)
-                for (int w = 0; w < 3; ++w) {
-                    int id = triangles[it].vertex_ids[w];
-                    bool seen = (id == tri.vertex_ids[0] || id == tri.vertex_ids[1] || id == tri.vertex_ids[2]);
-                    for (int c : cands) seen = seen || (c == id);
-                    if (!seen) {
-                        dists.push_back(norm3(P(id, 0) - tri.ref_centroid[0], P(id, 1) - tri.ref_centroid[1],
-                                              P(id, 2) - tri.ref_centroid[2]));
-                        cands.push_back(id);
-                    }
-                }
-        if (cands.size() < 3)
-            throw std::runtime_error("At least one search for patch nodes was exhausted without success (triangle " +
-                                     std::to_string(tri.id) + "): fewer than 3 candidate patch nodes.");
-        std::vector<size_t> order(dists.size());
-        for (size_t q = 0; q < order.size(); ++q) order[q] = q;
-        std::sort(order.begin(), order.end(), [&dists](const size_t& a, const size_t& b) { return dists[a] < dists[b]; });
-        tri.non_vertex_patch_nodes_ids[0] = cands[order[0]];
-        bool success = false;
-        for (size_t p = 1; p < std::min<size_t>(4, order.size()) && !success; ++p) {
-            tri.non_vertex_patch_nodes_ids[1] = cands[order[p]];
-            for (size_t q = 2; q < cands.size(); ++q) {
-                tri.non_vertex_patch_nodes_ids[2] = cands[order[q]];
-                int ids[6] = {tri.vertex_ids[0], tri.vertex_ids[1], tri.vertex_ids[2],
-                              tri.non_vertex_patch_nodes_ids[0], tri.non_vertex_patch_nodes_ids[1],
-                              tri.non_vertex_patch_nodes_ids[2]};
-                double sq = 0.0;
-                for (int n = 0; n < 6; ++n) {
-                    double dx = P(ids[n], 0) - tri.ref_centroid[0], dy = P(ids[n], 1) - tri.ref_centroid[1],
-                           dz = P(ids[n], 2) - tri.ref_centroid[2];
-                    sq += dx * dx + dy * dy + dz * dz;
-                }
-                double patch_size = std::sqrt(sq / 6.0);
-                double m[6][6];
-                for (int n = 0; n < 6; ++n) {
-                    double dx = P(ids[n], 0) - tri.ref_centroid[0];
-                    double dy = P(ids[n], 1) - tri.ref_centroid[1];
-                    m[0][n] = 1.0;
-                    m[1][n] = dx;
-                    m[2][n] = dy;
-                    m[3][n] = 0.5 * dx * dx;
-                    m[4][n] = dx * dy;
-                    m[5][n] = 0.5 * dy * dy;
-                }
-                bool accepted = false;
-                double block[6][3];
-                if (la::full_piv_rank<6>(m) == 6) {
-                    double inv[6][6];
-                    if (la::inverse_partial_piv<6>(m, inv)) {
-                        for (int r = 0; r < 6; ++r)
-                            for (int c = 0; c < 3; ++c) block[r][c] = inv[r][3 + c];
-                        double sigma = la::max_singular_value_6x3(block);
-                        double ratio = sigma * patch_size * patch_size / stuff.patch_mat_dimless_conditioning_thresh;
-                        accepted = ratio < 1.0;
-                    }
-                }
-                if (!accepted) {
-                    if (q == 2 && !tri.is_boundary) num_interior_retries += 1;
-                    continue;
-                }
-                for (int r = 0; r < 6; ++r)
-                    for (int c = 0; c < 3; ++c) tri.mat_for_patch_2nd_derivs[r][c] = block[r][c];
-                success = true;
-                break;
-            }
-        }
-        if (!success)
-            throw std::runtime_error(
-                "At least one search for patch nodes was exhausted without success (triangle " +
-                std::to_string(tri.id) +
-                "); all possible patch matrices in the search had a  condition number above the acceptance "
-                "threshold. Try increasing this threshold. If that does not solve the issue, or causes other "
-                "issues, either the patch node search will need to be extended, or you will need to use a nicer "
-                "mesh. Aborting.");
-    }
+        for (int t_index = t_begin; t_index < t_end; ++t_index)
+            fit_patch(t_index, nodes, P, triangles, stuff.patch_mat_dimless_conditioning_thresh, retries[worker]);
     });
     int num_interior_retries = 0;
     for (int r : retries) num_interior_retries += r;
-    log << "\nNumber of non-boundary triangles that had to search through \n"
-        << "multiple possible patch options to find one \nsatisfying the condition number "
-        << "criterion was " << num_interior_retries << ", \nwhich should not be a large proportion of the mesh's "
-        << "triangles." << std::endl;
+    log_patch_retries(log, num_interior_retries);
+}
+
+void deriv_coeffs_of(const Tri& tri, const DMat& P, double* c) {
+    double vpos[3][3];
+    for (int v = 0; v < 3; ++v)
+        for (int k = 0; k < 3; ++k) vpos[v][k] = P(tri.vertex_ids[v], k);
+    patch::first_derivative_weights(vpos, tri.ref_centroid, c);
+    for (int n = 0; n < 6; ++n)
+        for (int k = 0; k < 3; ++k) c[6 + 3 * n + k] = tri.mat_for_patch_2nd_derivs[n][k];
 }
 
 // source_files/calc_deriv_mats.cpp:46-136, kept as a dense per-triangle table
@@ -344,23 +335,8 @@ void calc_deriv_coeffs(std::vector<double>& coeffs, const DMat& P, const std::ve
                        const Stuff& stuff) {
     coeffs.assign(static_cast<size_t>(stuff.num_tris) * 24, 0.0);
     parallel_ranges((int)triangles.size(), setup_threads((int)triangles.size()), [&](int b, int e, int) {
-    for (int t_index = b; t_index < e; ++t_index) {
-        const Tri& tri = triangles[t_index];
-        double a[3][3], inv[3][3];
-        for (int v = 0; v < 3; ++v) {
-            a[v][0] = 1.0;
-            a[v][1] = P(tri.vertex_ids[v], 0) - tri.ref_centroid[0];
-            a[v][2] = P(tri.vertex_ids[v], 1) - tri.ref_centroid[1];
-        }
-        la::inverse3(a, inv);
-        double* c = &coeffs[static_cast<size_t>(tri.id) * 24];
-        for (int v = 0; v < 3; ++v) {
-            c[v] = inv[1][v];
-            c[3 + v] = inv[2][v];
-        }
-        for (int n = 0; n < 6; ++n)
-            for (int k = 0; k < 3; ++k) c[6 + 3 * n + k] = tri.mat_for_patch_2nd_derivs[n][k];
-    }
+        for (int t_index = b; t_index < e; ++t_index)
+            deriv_coeffs_of(triangles[t_index], P, &coeffs[static_cast<size_t>(triangles[t_index].id) * 24]);
     });
 }
 

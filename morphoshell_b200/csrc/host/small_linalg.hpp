@@ -11,21 +11,39 @@
 //                                       set_up_patch_fitting.cpp:243)
 //   * symmetric 3x3 eigen-decomposition by cyclic Jacobi rotations
 //                                      (SelfAdjointEigenSolver, calc_stresses.cpp:162)
+//
+// The routines compile for the host and, under nvcc, for the device as well
+// (the device set-up in setup.cu): the same operations in the same order,
+// so with contraction into fused multiply-adds off on the device both give
+// the same bits.
 #pragma once
 
-#include <algorithm>
 #include <cmath>
-#include <limits>
-#include <utility>
+
+#ifdef __CUDACC__
+#define MSB_HD __host__ __device__
+#else
+#define MSB_HD
+#endif
 
 namespace msb {
 namespace la {
+
+template <typename T>
+MSB_HD inline void swap_values(T& a, T& b) {
+    T t = a;
+    a = b;
+    b = t;
+}
+
+// The machine epsilon of double (std::numeric_limits<double>::epsilon()).
+constexpr double kEpsilon = 2.220446049250313080847e-16;
 
 // Rank of an n x n matrix (row-major, copied) by Gaussian elimination with
 // complete pivoting.  A pivot counts as non-zero when its magnitude exceeds
 // n * eps * (largest pivot met), the default threshold of a full-pivoting LU.
 template <int N>
-inline int full_piv_rank(const double (&a_in)[N][N]) {
+MSB_HD inline int full_piv_rank(const double (&a_in)[N][N]) {
     double a[N][N];
     for (int i = 0; i < N; ++i)
         for (int j = 0; j < N; ++j) a[i][j] = a_in[i][j];
@@ -37,14 +55,14 @@ inline int full_piv_rank(const double (&a_in)[N][N]) {
         double best = -1.0;
         for (int i = k; i < N; ++i)
             for (int j = k; j < N; ++j)
-                if (std::fabs(a[i][j]) > best) { best = std::fabs(a[i][j]); bi = i; bj = j; }
+                if (fabs(a[i][j]) > best) { best = fabs(a[i][j]); bi = i; bj = j; }
         if (best == 0.0) {
             npiv = k;
             break;
         }
         if (best > maxpivot) maxpivot = best;
-        if (bi != k) for (int j = 0; j < N; ++j) std::swap(a[k][j], a[bi][j]);
-        if (bj != k) for (int i = 0; i < N; ++i) std::swap(a[i][k], a[i][bj]);
+        if (bi != k) for (int j = 0; j < N; ++j) swap_values(a[k][j], a[bi][j]);
+        if (bj != k) for (int i = 0; i < N; ++i) swap_values(a[i][k], a[i][bj]);
         pivots[k] = a[k][k];
         for (int i = k + 1; i < N; ++i) {
             double f = a[i][k] / a[k][k];
@@ -52,17 +70,17 @@ inline int full_piv_rank(const double (&a_in)[N][N]) {
             a[i][k] = 0.0;
         }
     }
-    const double thresh = maxpivot * std::numeric_limits<double>::epsilon() * N;
+    const double thresh = maxpivot * kEpsilon * N;
     int rank = 0;
     for (int k = 0; k < npiv; ++k)
-        if (std::fabs(pivots[k]) > thresh) ++rank;
+        if (fabs(pivots[k]) > thresh) ++rank;
     return rank;
 }
 
 // Inverse of an n x n matrix by LU with partial (row) pivoting; returns false
 // when a pivot is exactly zero.
 template <int N>
-inline bool inverse_partial_piv(const double (&a_in)[N][N], double (&inv)[N][N]) {
+MSB_HD inline bool inverse_partial_piv(const double (&a_in)[N][N], double (&inv)[N][N]) {
     double lu[N][N];
     int perm[N];
     for (int i = 0; i < N; ++i) {
@@ -71,13 +89,13 @@ inline bool inverse_partial_piv(const double (&a_in)[N][N], double (&inv)[N][N])
     }
     for (int k = 0; k < N; ++k) {
         int p = k;
-        double best = std::fabs(lu[k][k]);
+        double best = fabs(lu[k][k]);
         for (int i = k + 1; i < N; ++i)
-            if (std::fabs(lu[i][k]) > best) { best = std::fabs(lu[i][k]); p = i; }
+            if (fabs(lu[i][k]) > best) { best = fabs(lu[i][k]); p = i; }
         if (best == 0.0) return false;
         if (p != k) {
-            for (int j = 0; j < N; ++j) std::swap(lu[k][j], lu[p][j]);
-            std::swap(perm[k], perm[p]);
+            for (int j = 0; j < N; ++j) swap_values(lu[k][j], lu[p][j]);
+            swap_values(perm[k], perm[p]);
         }
         for (int i = k + 1; i < N; ++i) {
             lu[i][k] /= lu[k][k];
@@ -100,7 +118,7 @@ inline bool inverse_partial_piv(const double (&a_in)[N][N], double (&inv)[N][N])
 }
 
 // 3x3 inverse by the adjugate: inv = adj(a) / det(a).
-inline void inverse3(const double (&a)[3][3], double (&inv)[3][3]) {
+MSB_HD inline void inverse3(const double (&a)[3][3], double (&inv)[3][3]) {
     double c00 = a[1][1] * a[2][2] - a[1][2] * a[2][1];
     double c01 = a[1][2] * a[2][0] - a[1][0] * a[2][2];
     double c02 = a[1][0] * a[2][1] - a[1][1] * a[2][0];
@@ -120,7 +138,7 @@ inline void inverse3(const double (&a)[3][3], double (&inv)[3][3]) {
 // Eigen-decomposition of a symmetric 3x3 matrix by cyclic Jacobi rotations.
 // Eigenvalues come out in ascending order; column k of vecs is the unit
 // eigenvector of vals[k].
-inline void sym_eig3(const double (&a_in)[3][3], double (&vals)[3], double (&vecs)[3][3]) {
+MSB_HD inline void sym_eig3(const double (&a_in)[3][3], double (&vals)[3], double (&vecs)[3][3]) {
     double a[3][3];
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) {
@@ -135,8 +153,8 @@ inline void sym_eig3(const double (&a_in)[3][3], double (&vals)[3], double (&vec
             for (int q = p + 1; q < 3; ++q) {
                 if (a[p][q] == 0.0) continue;
                 double theta = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
-                double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-                double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
                 for (int k = 0; k < 3; ++k) {
                     double akp = a[k][p], akq = a[k][q];
                     a[k][p] = c * akp - s * akq;
@@ -159,14 +177,14 @@ inline void sym_eig3(const double (&a_in)[3][3], double (&vals)[3], double (&vec
     for (int i = 0; i < 2; ++i)
         for (int j = 0; j < 2 - i; ++j)
             if (vals[j] > vals[j + 1]) {
-                std::swap(vals[j], vals[j + 1]);
-                for (int k = 0; k < 3; ++k) std::swap(vecs[k][j], vecs[k][j + 1]);
+                swap_values(vals[j], vals[j + 1]);
+                for (int k = 0; k < 3; ++k) swap_values(vecs[k][j], vecs[k][j + 1]);
             }
 }
 
 // Largest singular value of a 6x3 matrix: sqrt of the largest eigenvalue of
 // its 3x3 Gram matrix.
-inline double max_singular_value_6x3(const double (&m)[6][3]) {
+MSB_HD inline double max_singular_value_6x3(const double (&m)[6][3]) {
     double g[3][3];
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) {
@@ -176,7 +194,7 @@ inline double max_singular_value_6x3(const double (&m)[6][3]) {
         }
     double vals[3], vecs[3][3];
     sym_eig3(g, vals, vecs);
-    return std::sqrt(std::max(vals[2], 0.0));
+    return sqrt(vals[2] < 0.0 ? 0.0 : vals[2]);  // std::max(vals[2], 0.0), NaN kept
 }
 
 }  // namespace la
