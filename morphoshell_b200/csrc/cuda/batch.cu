@@ -129,6 +129,16 @@ __device__ __forceinline__ void batch_tri(const DevMesh& m, const int* __restric
                                           const double* __restrict__ pos, int t, const int (&ids)[6],
                                           const typename Real<MIXED>::T (&c)[24], double area, double c2, double s2,
                                           double cs, typename Real<MIXED>::T (&f)[18]) {
+    // The gathers go first: they do not depend on the instance, so they are
+    // in flight while its id and state load (a frozen instance's positions
+    // are read and not used).
+    double P[6][3];
+#pragma unroll
+    for (int sl = 0; sl < 6; ++sl) {
+        P[sl][0] = __ldg(pos + ids[sl]);
+        P[sl][1] = __ldg(pos + m.N + ids[sl]);
+        P[sl][2] = __ldg(pos + 2 * m.N + ids[sl]);
+    }
     const int inst = __ldg(tri_inst + t);
     const InstState& st = is[inst];
     if (is_frozen(st.status)) return;
@@ -137,13 +147,6 @@ __device__ __forceinline__ void batch_tri(const DevMesh& m, const int* __restric
     inst_material(q, m, t, mt);
     mt.area = area;
     lce_metric(c2, s2, cs, __dmul_rn(st.cur_lam, st.cur_lam), st.cur_pw, mt);
-    double P[6][3];
-#pragma unroll
-    for (int sl = 0; sl < 6; ++sl) {
-        P[sl][0] = __ldg(pos + ids[sl]);
-        P[sl][1] = __ldg(pos + m.N + ids[sl]);
-        P[sl][2] = __ldg(pos + 2 * m.N + ids[sl]);
-    }
     tri_forces<MIXED>(P, c, mt, q.nu, f);
 }
 
