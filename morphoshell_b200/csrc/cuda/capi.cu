@@ -252,12 +252,12 @@ ms_status build_tiles(ms_handle* h, const ms_mesh_desc* d) {
     return MS_OK;
 }
 
-// Largest nodes per tile of the node-tiled step (3 FP64 or 4 mixed blocks
+// Largest nodes per tile of the node-tiled step (3 FP64 or 5 mixed blocks
 // per SM; the tile count is a multiple of the resident blocks).  Measured on
 // the 1.8M-triangle disk: FP64 tiles of 1,023 nodes (two per block, 17.5 %
 // of the triangles on borders) beat 682 (three per block) by 3.4 % and 2,046
-// (one per block) by 17 %; mixed tiles of 768 nodes beat 512 and 1,535.  The
-// smallest tiles worth their border: 256 nodes.
+// (one per block) by 17 %; mixed tiles of 614 nodes at 5 blocks per SM beat
+// 410 at 5 and 768 at 4.  The smallest tiles worth their border: 256 nodes.
 #ifndef MSB_NT_NODES
 #define MSB_NT_NODES 1100
 #endif

@@ -40,12 +40,13 @@ using namespace tridev;
 using namespace tiles;
 
 // Resident blocks asked of the compiler (registers): FP64 at 3 per SM (168
-// registers; at 4 it spills and was measured slower), mixed at 4 (128).
+// registers; at 4 it spills and was measured slower), mixed at 5 (96, no
+// spills; 2.4 % faster than 4, while 6 spills and is slower).
 #ifndef MSB_NT_MINB
 #define MSB_NT_MINB 3
 #endif
 #ifndef MSB_NT_MINB_MIXED
-#define MSB_NT_MINB_MIXED 4
+#define MSB_NT_MINB_MIXED 5
 #endif
 
 template <int DIAL, bool MIXED>
