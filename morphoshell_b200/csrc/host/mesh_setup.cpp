@@ -34,6 +34,39 @@ double vmax(const std::vector<double>& v, size_t* arg = nullptr) {
     return *it;
 }
 
+// Threads for the per-triangle set-up loops: MORPHOSHELL_SETUP_THREADS, else
+// the hardware's; one for small meshes.
+int setup_threads(int n) {
+    if (n < 4096) return 1;
+    int t = (int)std::thread::hardware_concurrency();
+    if (const char* e = std::getenv("MORPHOSHELL_SETUP_THREADS")) t = std::atoi(e);
+    return std::max(1, std::min(t, 128));
+}
+
+// f(begin, end, worker) over [0, n) in contiguous ranges, one per thread.
+// The first exception (of the lowest range) is rethrown after all joined.
+template <typename F>
+void parallel_ranges(int n, int threads, F f) {
+    if (threads <= 1) {
+        f(0, n, 0);
+        return;
+    }
+    std::vector<std::thread> pool;
+    std::vector<std::exception_ptr> errs(threads);
+    const int chunk = (n + threads - 1) / threads;
+    for (int w = 0; w < threads; ++w)
+        pool.emplace_back([&, w]() {
+            try {
+                f(std::min(n, w * chunk), std::min(n, (w + 1) * chunk), w);
+            } catch (...) {
+                errs[w] = std::current_exception();
+            }
+        });
+    for (auto& t : pool) t.join();
+    for (auto& e : errs)
+        if (e) std::rethrow_exception(e);
+}
+
 }  // namespace
 
 // source_files/kahan_sum.cpp:32-49
@@ -56,32 +89,41 @@ void calc_mesh_info(std::vector<Node>& nodes, const DMat& P, std::vector<Tri>& t
     for (auto& node : nodes) node.incident_tri_ids.clear();
     for (const auto& tri : triangles)
         for (int v : tri.vertex_ids) nodes.at(v).incident_tri_ids.push_back(tri.id);
-    // 1-rings, sorted and unique.
-    for (auto& node : nodes) {
-        node.neighbour_node_ids.clear();
-        for (int t : node.incident_tri_ids)
-            for (int v : triangles[t].vertex_ids)
-                if (v != node.id) node.neighbour_node_ids.push_back(v);
-        std::sort(node.neighbour_node_ids.begin(), node.neighbour_node_ids.end());
-        node.neighbour_node_ids.erase(std::unique(node.neighbour_node_ids.begin(), node.neighbour_node_ids.end()),
-                                      node.neighbour_node_ids.end());
-    }
-    // Edge-sharing triangles.
-    for (auto& tri : triangles) {
-        std::vector<int> cand;
-        for (int v : tri.vertex_ids)
-            for (int t : nodes[v].incident_tri_ids)
-                if (t != tri.id) cand.push_back(t);
-        std::sort(cand.begin(), cand.end());
-        cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
-        tri.edge_sharing_tri_ids.clear();
-        for (int t : cand) {
-            int common = 0;
-            for (int a : tri.vertex_ids)
-                for (int b : triangles[t].vertex_ids) common += (a == b);
-            if (common == 2) tri.edge_sharing_tri_ids.push_back(t);
+    // 1-rings, sorted and unique (nodes independent: in parallel ranges).
+    const int nthreads = setup_threads(std::max((int)nodes.size(), (int)triangles.size()));
+    parallel_ranges((int)nodes.size(), nthreads, [&](int n0, int n1, int) {
+        for (int n = n0; n < n1; ++n) {
+            Node& node = nodes[n];
+            node.neighbour_node_ids.clear();
+            for (int t : node.incident_tri_ids)
+                for (int v : triangles[t].vertex_ids)
+                    if (v != node.id) node.neighbour_node_ids.push_back(v);
+            std::sort(node.neighbour_node_ids.begin(), node.neighbour_node_ids.end());
+            node.neighbour_node_ids.erase(
+                std::unique(node.neighbour_node_ids.begin(), node.neighbour_node_ids.end()),
+                node.neighbour_node_ids.end());
         }
-    }
+    });
+    // Edge-sharing triangles (triangles independent).
+    parallel_ranges((int)triangles.size(), nthreads, [&](int t0, int t1, int) {
+        std::vector<int> cand;
+        for (int ti = t0; ti < t1; ++ti) {
+            Tri& tri = triangles[ti];
+            cand.clear();
+            for (int v : tri.vertex_ids)
+                for (int t : nodes[v].incident_tri_ids)
+                    if (t != tri.id) cand.push_back(t);
+            std::sort(cand.begin(), cand.end());
+            cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+            tri.edge_sharing_tri_ids.clear();
+            for (int t : cand) {
+                int common = 0;
+                for (int a : tri.vertex_ids)
+                    for (int b : triangles[t].vertex_ids) common += (a == b);
+                if (common == 2) tri.edge_sharing_tri_ids.push_back(t);
+            }
+        }
+    });
     for (const auto& tri : triangles)
         if (tri.edge_sharing_tri_ids.size() < 1 || tri.edge_sharing_tri_ids.size() > 3)
             throw std::runtime_error(
@@ -101,25 +143,31 @@ void calc_mesh_info(std::vector<Node>& nodes, const DMat& P, std::vector<Tri>& t
                 edges.push_back(e);
             }
     stuff.num_edges = static_cast<int>(edges.size());
-    for (auto& e : edges) {
-        std::vector<int> a = nodes[e.node_ids[0]].incident_tri_ids, b = nodes[e.node_ids[1]].incident_tri_ids;
-        std::sort(a.begin(), a.end());
-        std::sort(b.begin(), b.end());
+    // Each edge's triangles: the common incident triangles of its ends (the
+    // incidence lists are in triangle order, so already sorted; edges
+    // independent).
+    parallel_ranges((int)edges.size(), nthreads, [&](int e0, int e1, int) {
         std::vector<int> common;
-        std::set_intersection(a.begin(), a.end(), b.begin(), b.end(), std::back_inserter(common));
-        if (common.size() == 1) {
-            e.is_boundary = true;
-            e.adjacent_tri_ids = common;
-        } else if (common.size() == 2) {
-            e.is_boundary = false;
-            e.adjacent_tri_ids = common;
-        } else {
-            throw std::runtime_error(
-                "Something has gone very wrong in calc_edges, because the nodes at each end of an edge "
-                "should have either one or two incident triangles in common, but the code thinks it's "
-                "found an exception. Investigate!");
+        for (int ei = e0; ei < e1; ++ei) {
+            Edge& e = edges[ei];
+            const std::vector<int>& a = nodes[e.node_ids[0]].incident_tri_ids;
+            const std::vector<int>& b = nodes[e.node_ids[1]].incident_tri_ids;
+            common.clear();
+            std::set_intersection(a.begin(), a.end(), b.begin(), b.end(), std::back_inserter(common));
+            if (common.size() == 1) {
+                e.is_boundary = true;
+                e.adjacent_tri_ids = common;
+            } else if (common.size() == 2) {
+                e.is_boundary = false;
+                e.adjacent_tri_ids = common;
+            } else {
+                throw std::runtime_error(
+                    "Something has gone very wrong in calc_edges, because the nodes at each end of an edge "
+                    "should have either one or two incident triangles in common, but the code thinks it's "
+                    "found an exception. Investigate!");
+            }
         }
-    }
+    });
     std::vector<int> cursor(stuff.num_tris, 0);
     for (const auto& e : edges)
         for (int t : e.adjacent_tri_ids) {
@@ -198,42 +246,6 @@ void calc_mesh_info(std::vector<Node>& nodes, const DMat& P, std::vector<Tri>& t
             tri.ref_centroid[k] = (P(tri.vertex_ids[0], k) + P(tri.vertex_ids[1], k) + P(tri.vertex_ids[2], k)) / 3.0;
 }
 
-namespace {
-
-// Threads for the per-triangle set-up loops: MORPHOSHELL_SETUP_THREADS, else
-// the hardware's; one for small meshes.
-int setup_threads(int n) {
-    if (n < 4096) return 1;
-    int t = (int)std::thread::hardware_concurrency();
-    if (const char* e = std::getenv("MORPHOSHELL_SETUP_THREADS")) t = std::atoi(e);
-    return std::max(1, std::min(t, 128));
-}
-
-// f(begin, end, worker) over [0, n) in contiguous ranges, one per thread.
-// The first exception (of the lowest range) is rethrown after all joined.
-template <typename F>
-void parallel_ranges(int n, int threads, F f) {
-    if (threads <= 1) {
-        f(0, n, 0);
-        return;
-    }
-    std::vector<std::thread> pool;
-    std::vector<std::exception_ptr> errs(threads);
-    const int chunk = (n + threads - 1) / threads;
-    for (int w = 0; w < threads; ++w)
-        pool.emplace_back([&, w]() {
-            try {
-                f(std::min(n, w * chunk), std::min(n, (w + 1) * chunk), w);
-            } catch (...) {
-                errs[w] = std::current_exception();
-            }
-        });
-    for (auto& t : pool) t.join();
-    for (auto& e : errs)
-        if (e) std::rethrow_exception(e);
-}
-
-}  // namespace
 
 void log_patch_retries(Log& log, int num_interior_retries) {
     log << "\nNumber of non-boundary triangles that had to search through \n"
