@@ -91,3 +91,17 @@ def test_layout_sliced_order_sizes(workdir):
         fixed = 128 * (6 * 4 + 24 * (4 if prec else 8) + 4 * 8)
         stage = -(-3 * slc * (4 if prec else 8) // 128) * 128
         assert info["pipe_shared_bytes"] > 2 * fixed + 2 * stage + 2 * 128 * 8 * 8 + 24 * 1024
+
+
+def test_layout_same_with_one_thread_and_many(workdir, monkeypatch):
+    """The host layout runs one thread per range of tiles; the plan it
+    describes does not depend on the thread count."""
+    from morphoshell_b200 import MS_PRECISION_MIXED, node_tile_layout
+    m = make_model(workdir, "disk18k")
+    P = m.tables()["patch_ids"]
+    for prec in (0, MS_PRECISION_MIXED):
+        monkeypatch.setenv("MORPHOSHELL_SETUP_THREADS", "1")
+        one = node_tile_layout(P, m.num_nodes, 300, prec)
+        monkeypatch.setenv("MORPHOSHELL_SETUP_THREADS", "7")
+        many = node_tile_layout(P, m.num_nodes, 300, prec)
+        assert one == many
