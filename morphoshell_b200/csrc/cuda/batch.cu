@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(BLOCK) k_batch_tri(const DevMesh m, const Clus
 template <bool MIXED>
 __device__ __forceinline__ void batch_tri(const DevMesh& m, const int* __restrict__ tri_inst,
                                           const InstParams* __restrict__ ip, const InstState* __restrict__ is,
-                                          const double* __restrict__ pos, int t, const int (&ids)[6],
+                                          const double* __restrict__ pos, int t, int inst_hint, const int (&ids)[6],
                                           const typename Real<MIXED>::T (&c)[24], double area, double c2, double s2,
                                           double cs, typename Real<MIXED>::T (&f)[18]) {
     // The gathers go first: they do not depend on the instance, so they are
@@ -139,7 +139,7 @@ __device__ __forceinline__ void batch_tri(const DevMesh& m, const int* __restric
         P[sl][1] = __ldg(pos + m.N + ids[sl]);
         P[sl][2] = __ldg(pos + 2 * m.N + ids[sl]);
     }
-    const int inst = __ldg(tri_inst + t);
+    const int inst = inst_hint >= 0 ? inst_hint : __ldg(tri_inst + t);
     const InstState& st = is[inst];
     if (is_frozen(st.status)) return;
     const InstParams& q = ip[inst];
@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(kTile) k_batch_tri_tiles(const DevMesh m, cons
     tiles::tile_loop<MIXED>(
         m.T, tl, out, err,
         [&](int t, const int (&ids)[6], const R (&c)[24], double area, double c2, double s2, double cs, R (&f)[18]) {
-            batch_tri<MIXED>(m, tri_inst, ip, is, pos, t, ids, c, area, c2, s2, cs, f);
+            batch_tri<MIXED>(m, tri_inst, ip, is, pos, t, -1, ids, c, area, c2, s2, cs, f);
         });
 }
 
@@ -251,9 +251,8 @@ __global__ void __launch_bounds__(kTile, MIXED ? MSB_NT_MINB_MIXED : MSB_NT_MINB
     const double* pos = pos_buf(s, parity);
     tiles::node_tile_walk<MIXED>(
         q, m.N, true, err,
-        [&](int t, const int (&ids)[6], const R (&c)[24], double area, double c2, double s2, double cs, R (&f)[18]) {
-            batch_tri<MIXED>(m, tri_inst, ip, is, pos, t, ids, c, area, c2, s2, cs, f);
-        },
+        [&](int t, int inst, const int (&ids)[6], const R (&c)[24], double area, double c2, double s2, double cs,
+            R (&f)[18]) { batch_tri<MIXED>(m, tri_inst, ip, is, pos, t, inst, ids, c, area, c2, s2, cs, f); },
         [&](int n, double Fx, double Fy, double Fz) {
             const int inst = __ldg(node_inst + n);
             if (!is_frozen(is[inst].status)) batch_node_core(m, s, ip[inst], is, inst, n, Fx, Fy, Fz, fnorm, vnorm, parity);
@@ -262,13 +261,15 @@ __global__ void __launch_bounds__(kTile, MIXED ? MSB_NT_MINB_MIXED : MSB_NT_MINB
 
 // The tables part of the node-tiled records (ids, weights, area and
 // director trigonometry, field-major per chunk), gathered from the union's
-// per-triangle tables: the bytes fill_node_tile_records writes on the host.
-// One block per chunk, one thread per slot; empty slots get zeros.
+// per-triangle tables: the bytes fill_node_tile_records writes on the host;
+// and each slot's instance (the plan's chunk_tag, which the walk loads with
+// the tables).  One block per chunk, one thread per slot; empty slots get
+// zeros.
 template <bool MIXED>
 __global__ void __launch_bounds__(kTile)
     k_fill_node_tile_tables(unsigned char* __restrict__ rec, size_t stride, const int* __restrict__ chunk_tri,
                             const int4* __restrict__ tri_idx, const typename Real<MIXED>::T* __restrict__ coef,
-                            const double4* __restrict__ aux) {
+                            const double4* __restrict__ aux, int* __restrict__ chunk_inst) {
     using R = typename Real<MIXED>::T;
     using L = tiles::TileLayout<MIXED>;
     const int c = blockIdx.x, i = threadIdx.x;
@@ -279,6 +280,7 @@ __global__ void __launch_bounds__(kTile)
     const int t = chunk_tri[(size_t)c * kTile + i];
     if (t >= 0) {
         const int4 a = tri_idx[2 * (size_t)t], b = tri_idx[2 * (size_t)t + 1];
+        chunk_inst[(size_t)c * kTile + i] = b.w;  // the triangle's instance
         const int id[6] = {a.x, a.y, a.z, a.w, b.x, b.y};
 #pragma unroll
         for (int k = 0; k < 6; ++k) ids[k * kTile + i] = id[k];
@@ -290,6 +292,7 @@ __global__ void __launch_bounds__(kTile)
         ax[2 * kTile + i] = x.z;
         ax[3 * kTile + i] = x.w;
     } else {
+        chunk_inst[(size_t)c * kTile + i] = 0;
 #pragma unroll
         for (int k = 0; k < 6; ++k) ids[k * kTile + i] = 0;
 #pragma unroll
@@ -596,9 +599,10 @@ ms_status plan_from_layout(ms_batch* b, const NodeTileLayout& L, int NT, int blo
         return MS_OK;
     };
     unsigned char* d_rec;
-    int *d_tc, *d_ctri;
+    int *d_tc, *d_ctri, *d_tag;
     unsigned* d_bytes;
     MB_TRY(dal(reinterpret_cast<void**>(&d_rec), L.stride * (size_t)L.C));
+    MB_TRY(dal(reinterpret_cast<void**>(&d_tag), sizeof(int) * ctri.size()));
     MB_TRY(dal(reinterpret_cast<void**>(&d_tc), sizeof(int) * L.tile_chunk.size()));
     MB_TRY(dal(reinterpret_cast<void**>(&d_bytes), sizeof(unsigned) * L.bytes.size()));
     MB_TRY(dal(reinterpret_cast<void**>(&d_ctri), sizeof(int) * ctri.size()));
@@ -610,10 +614,10 @@ ms_status plan_from_layout(ms_batch* b, const NodeTileLayout& L, int NT, int blo
     if (L.C > 0) {
         if (b->precision == MS_PRECISION_MIXED)
             k_fill_node_tile_tables<true><<<L.C, kTile, 0, b->stream>>>(d_rec, L.stride, d_ctri, b->p.tri_idx,
-                                                                        b->p.coef_aos_f, b->p.tri_aux);
+                                                                        b->p.coef_aos_f, b->p.tri_aux, d_tag);
         else
             k_fill_node_tile_tables<false><<<L.C, kTile, 0, b->stream>>>(d_rec, L.stride, d_ctri, b->p.tri_idx,
-                                                                         b->p.coef_aos, b->p.tri_aux);
+                                                                         b->p.coef_aos, b->p.tri_aux, d_tag);
         MB_CUDA(b, cudaGetLastError());
         MB_CUDA(b, cudaStreamSynchronize(b->stream));
     }
@@ -628,6 +632,7 @@ ms_status plan_from_layout(ms_batch* b, const NodeTileLayout& L, int NT, int blo
     q.tile_chunk = d_tc;
     q.chunk_bytes = d_bytes;
     q.chunk_tri = d_ctri;
+    q.chunk_tag = d_tag;
     return MS_OK;
 }
 

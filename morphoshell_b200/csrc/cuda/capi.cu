@@ -363,6 +363,7 @@ ms_status build_node_tiles(ms_handle* h, const ms_mesh_desc* d, const std::vecto
     q.tile_chunk = d_tile_chunk;
     q.chunk_bytes = d_bytes;
     q.chunk_tri = d_ctri;
+    q.chunk_tag = nullptr;
     h->d_nt_rec = d_rec;
     // One equilibrium partial per block.
     const int parts = std::min(K, std::max(q.grid, q.grid_pipe));

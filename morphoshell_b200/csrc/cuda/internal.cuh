@@ -171,6 +171,7 @@ struct NodeTilePlan {
     const int* tile_chunk;           // [ntiles + 1] first chunk of each tile
     const unsigned* chunk_bytes;     // [nchunks] bytes to copy of each record (multiple of 16)
     const int* chunk_tri;            // [nchunks][kTile] triangle of each slot, -1 past the chunk's end
+    const int* chunk_tag;            // [nchunks][kTile] the caller's value per slot (a batch: the instance), or null
     int slc;                         // entries of the sliced staging area (NodeTileLayout::slc_max)
 };
 

@@ -2,9 +2,10 @@
 // (node_tiles.cu) and the batched one (batch.cu).  A block takes node tiles
 // blockIdx.x, then every gridDim.x-th; for each tile it walks the chunk
 // records of the tile's triangle list (NodeTilePlan), calls
-//   tri(t, ids, c, area, c2, s2, cs, f)
-// for every live triangle slot (t its triangle when need_t, else 0; f the 18
-// contributions, zero on entry), adds the contributions to the tile's node
+//   tri(t, tag, ids, c, area, c2, s2, cs, f)
+// for every live triangle slot (t its triangle when need_t, else 0; tag the
+// plan's per-slot value, chunk_tag, or 0; f the 18 contributions, zero on
+// entry), adds the contributions to the tile's node
 // accumulators run by run in ascending triangle order, and after the tile's
 // last chunk calls
 //   node(n, Fx, Fy, Fz)
@@ -77,10 +78,11 @@ struct SlotTables {
     int ids[6];
     R cf[24];
     double area, c2, s2, cs;
-    int t;
+    int t, tag;
 
     __device__ __forceinline__ void load(const unsigned char* __restrict__ rec, int i, int c, bool need_t,
-                                         const int* __restrict__ chunk_tri, uint64_t pol) {
+                                         const int* __restrict__ chunk_tri, const int* __restrict__ chunk_tag,
+                                         uint64_t pol) {
         using L = TileLayout<MIXED>;
         const int* sid = reinterpret_cast<const int*>(rec);
         const R* scoef = reinterpret_cast<const R*>(rec + L::ids);
@@ -95,6 +97,7 @@ struct SlotTables {
         cs = ld_stream(saux + 3 * kTile + i, pol);
         // Empty slots of a chunk hold -1 here; they are never computed.
         t = need_t ? __ldg(chunk_tri + (size_t)c * kTile + i) : 0;
+        tag = chunk_tag ? __ldg(chunk_tag + (size_t)c * kTile + i) : 0;
     }
 };
 
@@ -133,7 +136,7 @@ __device__ __forceinline__ void node_tile_walk(const NodeTilePlan& q, int N, boo
     int c = __ldg(q.tile_chunk + tile);
     if (i == 0) fetch(c, 0);
     SlotTables<MIXED> tb;
-    tb.load(q.rec + (size_t)c * q.stride, i, c, need_t, q.chunk_tri, pol);
+    tb.load(q.rec + (size_t)c * q.stride, i, c, need_t, q.chunk_tri, q.chunk_tag, pol);
     uint32_t phase = 0u;
     int slot = 0;  // node-section slot of the current chunk
     for (;;) {
@@ -159,12 +162,12 @@ __device__ __forceinline__ void node_tile_walk(const NodeTilePlan& q, int N, boo
             R f[18];
 #pragma unroll
             for (int j = 0; j < 18; ++j) f[j] = R(0);
-            if (i < hd.z) tri(tb.t, tb.ids, tb.cf, tb.area, tb.c2, tb.s2, tb.cs, f);
+            if (i < hd.z) tri(tb.t, tb.tag, tb.ids, tb.cf, tb.area, tb.c2, tb.s2, tb.cs, f);
 #pragma unroll
             for (int k = 0; k < 18; ++k) stage[k * kTile + i] = f[k];
             __syncthreads();
             // The next chunk's tables load while this chunk's runs add up.
-            if (nc >= 0) tb.load(q.rec + (size_t)nc * q.stride, i, nc, need_t, q.chunk_tri, pol);
+            if (nc >= 0) tb.load(q.rec + (size_t)nc * q.stride, i, nc, need_t, q.chunk_tri, q.chunk_tag, pol);
             // Runs: one node's entries of this chunk each, distinct nodes, so
             // the runs of a chunk add in parallel without conflicts.  Staging
             // is field-major: component k of patch slot sl of the chunk's

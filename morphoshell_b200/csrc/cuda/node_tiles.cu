@@ -69,7 +69,8 @@ __global__ void __launch_bounds__(kTile, MIXED ? MSB_NT_MINB_MIXED : MSB_NT_MINB
     int fnode = INT_MAX, vnode = INT_MAX;
     node_tile_walk<MIXED>(
         q, m.N, need_t, &s.err->flag,
-        [&](int t, const int (&ids)[6], const R (&cf)[24], double area, double c2, double s2, double cs, R (&f)[18]) {
+        [&](int t, int, const int (&ids)[6], const R (&cf)[24], double area, double c2, double s2, double cs,
+            R (&f)[18]) {
             tile_tri<DIAL, MIXED>(m, p, pos, dial, lam, pw, t, ids, cf, area, c2, s2, cs, f);
         },
         [&](int n, double Fx, double Fy, double Fz) {
