@@ -173,22 +173,39 @@ __global__ void __launch_bounds__(kTile) k_batch_tri_tiles(const DevMesh m, cons
 // Everything after the deformation-force sum for node n of a live instance:
 // node_finish with the instance's scalars, |F| and |v| to fnorm / vnorm on
 // the instance's check steps, a guard trip into the instance's guard key.
+// A node's state for the update: position and velocity from buffer
+// `parity`, mass, constraint flag (independent of its instance, so these
+// loads can be in flight while the instance's state loads).
+__device__ __forceinline__ NodeIn batch_node_load(const DevMesh& m, const DevState& s, int n, int parity) {
+    const int N = m.N;
+    const double* pos = pos_buf(s, parity);
+    const double* vel = vel_buf(s, parity);
+    NodeIn in;
+    in.px = pos[n];
+    in.py = pos[N + n];
+    in.pz = pos[2 * N + n];
+    in.vx = vel[n];
+    in.vy = vel[N + n];
+    in.vz = vel[2 * N + n];
+    in.mass = __ldg(m.mass + n);
+    in.fixed = __ldg(m.fixed + n);
+    return in;
+}
+
 __device__ __forceinline__ void batch_node_core(const DevMesh& m, const DevState& s, const InstParams& q,
-                                                InstState* __restrict__ is, int inst, int n, double Fx, double Fy,
-                                                double Fz, double* __restrict__ fnorm, double* __restrict__ vnorm,
-                                                int parity) {
+                                                InstState* __restrict__ is, int inst, int n, const NodeIn& in,
+                                                double Fx, double Fy, double Fz, double* __restrict__ fnorm,
+                                                double* __restrict__ vnorm, int parity) {
     const int N = m.N;
     const double damping = is[inst].damping;
     const int check = is[inst].check_now;
-    const double* pos = pos_buf(s, parity);
-    const double* vel = vel_buf(s, parity);
-    const double vx = vel[n], vy = vel[N + n], vz = vel[2 * N + n];
-    const double mass = __ldg(m.mass + n);
+    const double vx = in.vx, vy = in.vy, vz = in.vz;
+    const double mass = in.mass;
     const double dm = -damping * mass / q.rho_hh;
     Fx += dm * vx;
     Fy += dm * vy;
     Fz += dm * vz;
-    if (__ldg(m.fixed + n)) Fx = Fy = Fz = 0.0;
+    if (in.fixed) Fx = Fy = Fz = 0.0;
     if (check) {
         fnorm[n] = sqrt(Fx * Fx + Fy * Fy + Fz * Fz);
         vnorm[n] = sqrt(vx * vx + vy * vy + vz * vz);
@@ -202,9 +219,9 @@ __device__ __forceinline__ void batch_node_core(const DevMesh& m, const DevState
     const double nvx = vx + k2 * Fx, nvy = vy + k2 * Fy, nvz = vz + k2 * Fz;
     double* npos = pos_buf(s, parity ^ 1);
     double* nvel = vel_buf(s, parity ^ 1);
-    npos[n] = pos[n] + q.dt * nvx;
-    npos[N + n] = pos[N + n] + q.dt * nvy;
-    npos[2 * N + n] = pos[2 * N + n] + q.dt * nvz;
+    npos[n] = in.px + q.dt * nvx;
+    npos[N + n] = in.py + q.dt * nvy;
+    npos[2 * N + n] = in.pz + q.dt * nvz;
     nvel[n] = nvx;
     nvel[N + n] = nvy;
     nvel[2 * N + n] = nvz;
@@ -229,7 +246,7 @@ __global__ void __launch_bounds__(BLOCK) k_batch_node(const DevMesh m, const Dev
     if constexpr (MIXED) gather_sell<float>(m, m.contrib_f, n, Fx, Fy, Fz);
     else gather_sell<double>(m, s.contrib, n, Fx, Fy, Fz);
     if (!active) return;
-    batch_node_core(m, s, ip[inst], is, inst, n, Fx, Fy, Fz, fnorm, vnorm, parity);
+    batch_node_core(m, s, ip[inst], is, inst, n, batch_node_load(m, s, n, parity), Fx, Fy, Fz, fnorm, vnorm, parity);
 }
 
 // The whole step of the union in one kernel (node_tile_walk.cuh): a block
@@ -254,8 +271,10 @@ __global__ void __launch_bounds__(kTile, MIXED ? MSB_NT_MINB_MIXED : MSB_NT_MINB
         [&](int t, int inst, const int (&ids)[6], const R (&c)[24], double area, double c2, double s2, double cs,
             R (&f)[18]) { batch_tri<MIXED>(m, tri_inst, ip, is, pos, t, inst, ids, c, area, c2, s2, cs, f); },
         [&](int n, double Fx, double Fy, double Fz) {
+            const NodeIn in = batch_node_load(m, s, n, parity);  // read for frozen instances too, then unused
             const int inst = __ldg(node_inst + n);
-            if (!is_frozen(is[inst].status)) batch_node_core(m, s, ip[inst], is, inst, n, Fx, Fy, Fz, fnorm, vnorm, parity);
+            if (!is_frozen(is[inst].status))
+                batch_node_core(m, s, ip[inst], is, inst, n, in, Fx, Fy, Fz, fnorm, vnorm, parity);
         });
 }
 
