@@ -159,9 +159,10 @@ ms_status ms_advance_dynamics(ms_handle* h, double timestep, double damping_fact
  * space is a static device array inside this library, sized for at most
  * 65,536 nodes and 65,536 triangles (about 11.5 MB that every GPU loading
  * the library keeps until exit); larger meshes return
- * MS_ERR_INVALID_ARGUMENT with the reason in err.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress); make
- * that first call before any stream capture.  All calls share the array:
+ * MS_ERR_INVALID_ARGUMENT with the reason in err.  Every call looks up that
+ * array's device address in the current context (cudaGetSymbolAddress; the
+ * first call on a device also loads the library's device code, so make it
+ * before any stream capture).  All calls share the array:
  * calls that overlap on the GPU race, so serialise them.  Runs on `stream`
  * (a cudaStream_t, NULL for the default stream) and returns after the forces
  * are written (it waits for the stream, to check the patch ids).  A CUDA

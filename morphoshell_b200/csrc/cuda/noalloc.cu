@@ -25,7 +25,6 @@
 // contributions are added in ascending triangle order, as in the main path.
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 
 #include "../../../include/morphoshell_gpu.h"
 #include "tri_physics.cuh"
@@ -45,23 +44,14 @@ struct Scratch {
 
 static __device__ __align__(256) unsigned char ms_noalloc_scratch[sizeof(Scratch)];
 
-// Device address of the scratch array, looked up once per device.
-std::mutex g_mu;
-void* g_addr[256];
-
+// Device address of the scratch array in the current context, looked up on
+// every call (a table lookup once the module is loaded), so that an address
+// never outlives the context it belongs to, e.g. across cudaDeviceReset.
 cudaError_t scratch_address(Scratch** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, ms_noalloc_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= 256) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, ms_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_addr[dev] = p;
-    }
-    *out = static_cast<Scratch*>(g_addr[dev]);
+    *out = static_cast<Scratch*>(p);
     return cudaSuccess;
 }
 
