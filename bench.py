@@ -517,8 +517,8 @@ def time_to_equilibrium(device: int, seed: int = 11) -> dict:
     sin(k theta + phi_k), lambda ~ U(0.8, 1.2)) on a 0.06-spacing disk train
     the tensor-core network; 16 held-out fields then run from both starts in
     one batch each.  Four short dial phases and thresholds 1e-5 / 1e-4 keep
-    it to about a minute (BASELINE configs 4 and 5 ask for 4096 fields on the
-    18k disk and 64 on the 1.8M disk)."""
+    it to about a minute (the full-scale studies are 4096 fields on the 18k
+    disk and 64 on the 1.8M disk)."""
     import tempfile as _tf
 
     from morphoshell_b200 import Mlp, Model, meshgen, warmstart
@@ -545,7 +545,7 @@ def time_to_equilibrium(device: int, seed: int = 11) -> dict:
             "same_shape_fraction": r["same_shape_fraction"],
             "energy_ratio_learned_to_plain": r["learned_energy_median"] / r["plain_energy_median"],
             "loss_first_last": [float(losses[0]), float(losses[-1])], "total_s": time.time() - t0,
-            "note": "reduced-scale stand-in for BASELINE configs 4/5; same_shape_fraction is the share of held-out "
+            "note": "reduced-scale stand-in for the 4096-field 18k-disk and 64-field 1.8M-disk studies; same_shape_fraction is the share of held-out "
                     "fields whose learned-start equilibrium is the plain-start one"}
 
 
