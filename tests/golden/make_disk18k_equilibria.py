@@ -4,7 +4,7 @@ unmodified by oracle/build.py, with do_dialling.cpp's protocol-3 block
 switched on) run on the 18k-triangle disk to its first equilibrium at dial
 factor 1.
 
-    python tests/golden/make_cfg1_equilibria.py [--reuse RUN_DIR]
+    python tests/golden/make_disk18k_equilibria.py [--reuse RUN_DIR]
 
 Workload: ``meshgen.write_workload(dir, "disk18k", **SETTINGS)`` -- unit disk,
 jittered hex spacing 0.02 (9,201 nodes, 18,086 triangles), azimuthal
@@ -73,7 +73,7 @@ def parse_vtk(path):
 def run_reference(threads):
     import oracle
     from morphoshell_b200 import meshgen
-    d = tempfile.mkdtemp(prefix="cfg1_")
+    d = tempfile.mkdtemp(prefix="disk18k_eq_")
     meshgen.write_workload(d, "disk18k", **SETTINGS)
     out = os.path.join(d, "output_using_disk18k_settings.txt")
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))

@@ -2,7 +2,7 @@
 functions (oracle/_ref/libmorpho_ref.so, compiled from its source by
 oracle/build.py) run for 10^4 fixed dialling steps on the 1.8M-triangle disk.
 
-    python tests/golden/make_cfg2_trajectory.py [--threads K] [--steps 10000]
+    python tests/golden/make_disk1p8m_trajectory.py [--threads K] [--steps 10000]
 
 Workload: ``meshgen.write_workload(dir, "disk1p8m")`` -- unit disk, jittered
 hex spacing 0.002 (908,139 nodes, 1,813,134 triangles), wavy azimuthal
@@ -73,7 +73,7 @@ def main() -> None:
     ap.add_argument("--kind", default="ref", choices=["ref", "orc"])
     a = ap.parse_args()
     t0 = time.time()
-    d = tempfile.mkdtemp(prefix="cfg2_")
+    d = tempfile.mkdtemp(prefix="disk1p8m_traj_")
     st, vtk = meshgen.write_workload(d, "disk1p8m")
     m = Model(st, vtk, quiet=True)
     s = m.scalars

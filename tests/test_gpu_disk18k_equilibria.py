@@ -2,7 +2,7 @@
 the reference's own executable.
 
 tests/golden/disk18k_equilibria.npz (written by
-tests/golden/make_cfg1_equilibria.py) holds the reference executable's run
+tests/golden/make_disk18k_equilibria.py) holds the reference executable's run
 of this workload -- every equilibrium up to the first at dial factor 1, with
 the positions written at each and the last output file's fields.  This
 project's command-line driver runs the same settings and mesh (host set-up,
@@ -32,9 +32,9 @@ POINT_TOL = 1e-9    # of the largest coordinate (the disk's radius)
 FIELD_TOL = 1e-10   # norm-wise per field (the last equilibrium: 2e-11 measured)
 
 
-def test_cfg1_equilibria_match_reference_executable(tmp_path):
+def test_disk18k_equilibria_match_reference_executable(tmp_path):
     sys.path.insert(0, os.path.join(HERE, "golden"))
-    from make_cfg1_equilibria import SETTINGS, equilibria, parse_vtk
+    from make_disk18k_equilibria import SETTINGS, equilibria, parse_vtk
     from morphoshell_b200 import meshgen
     from morphoshell_b200.build import EXE
     g = np.load(FIXTURE)

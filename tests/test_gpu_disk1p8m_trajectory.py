@@ -3,7 +3,7 @@
 
 The reference's run is too long to repeat here (about half an hour of CPU on
 all host threads), so it is a committed fixture, tests/golden/disk1p8m_traj.npz,
-written by tests/golden/make_cfg2_trajectory.py from the reference's own
+written by tests/golden/make_disk1p8m_trajectory.py from the reference's own
 per-step functions (compiled from its source).  The fixture holds a seeded
 sample of 65,536 nodes of the final state, the global maxima of the last step
 (max |F|, max |v| and their nodes) and the largest |z| with its node; the
@@ -40,13 +40,13 @@ MIXED_SHAPE_TOL = 1e-5  # of the mesh size (diameter 2)
 
 
 @pytest.fixture(scope="module")
-def cfg2(tmp_path_factory):
+def disk1p8m_run(tmp_path_factory):
     import sys
     sys.path.insert(0, os.path.join(HERE, "golden"))
-    from make_cfg2_trajectory import dial_schedule, fingerprint, sample_nodes
+    from make_disk1p8m_trajectory import dial_schedule, fingerprint, sample_nodes
     from morphoshell_b200 import Model, meshgen
     g = np.load(FIXTURE)
-    d = str(tmp_path_factory.mktemp("cfg2"))
+    d = str(tmp_path_factory.mktemp("disk1p8m"))
     st, vtk = meshgen.write_workload(d, "disk1p8m")
     m = Model(st, vtk, quiet=True)
     fp = fingerprint(m)
@@ -90,8 +90,8 @@ def _gpu_forces(gl, x, v, dial):
 
 
 @pytest.mark.parametrize("path", [4, 3, 2])
-def test_cfg2_1e4_steps_against_reference(cfg2, path):
-    m, g, idx, dials = cfg2
+def test_disk1p8m_1e4_steps_against_reference(disk1p8m_run, path):
+    m, g, idx, dials = disk1p8m_run
     N = m.num_nodes
     gl, rep = _run(m, dials, path=path)
     x, v = gl.download()
@@ -124,11 +124,11 @@ def test_cfg2_1e4_steps_against_reference(cfg2, path):
     gl.close()
 
 
-def test_cfg2_forces_on_a_deformed_state(cfg2):
+def test_disk1p8m_forces_on_a_deformed_state(disk1p8m_run):
     """Per-step deformation forces of the 1.8M-triangle mesh on a smooth,
     well-conditioned deformed state, within 1e-12 of the oracle."""
     from morphoshell_b200 import GpuLoop
-    m = cfg2[0]
+    m = disk1p8m_run[0]
     x, v = deformed_state(m, seed=41, amp=0.02)
     s = m.scalars
     a_info, b_info = m.programmed()
@@ -142,10 +142,10 @@ def test_cfg2_forces_on_a_deformed_state(cfg2):
     assert err < FORCE_RTOL
 
 
-def test_cfg2_mixed_precision_error_against_reference(cfg2):
+def test_disk1p8m_mixed_precision_error_against_reference(disk1p8m_run):
     """The mixed path over the same 10^4 steps: final positions against the
     reference's, as a fraction of the mesh size (the unit disk, diameter 2)."""
-    m, g, idx, dials = cfg2
+    m, g, idx, dials = disk1p8m_run
     N = m.num_nodes
     gl, _ = _run(m, dials, precision=1)
     x, _ = gl.download()

@@ -24,7 +24,7 @@ from conftest import deformed_state, make_model, protocol_inputs, rel_err
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 # The per-function golden vectors (make_golden.py); disk1p8m_traj.npz is the
-# GPU trajectory fixture of tests/test_gpu_cfg2.py.
+# GPU trajectory fixture of tests/test_gpu_disk1p8m_trajectory.py.
 GOLDEN = sorted(glob.glob(os.path.join(HERE, "golden", "*_p[0-9].npz")))
 
 
