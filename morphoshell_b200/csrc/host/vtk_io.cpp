@@ -2,6 +2,12 @@
 //   input  : source_files/read_vtk_data.cpp:65-371 (mesh + programmed fields)
 //            and :380-445 (ansatz, an output file of an earlier run)
 //   output : source_files/write_output.cpp:46-170 (also the restart format)
+#include <cerrno>
+#include <climits>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
 #include <iomanip>
 #include <limits>
 
@@ -11,9 +17,194 @@ namespace msb {
 
 namespace {
 
-constexpr std::streamsize kMax = std::numeric_limits<std::streamsize>::max();
+// The whole file in memory, read with the std::istream operations the
+// reference's reader uses (operator>> for words, int, bool, double;
+// ignore(n, delim); ignore(1)) and their "C"-locale semantics: whitespace
+// is skipped before a formatted read; a read that finds nothing it can
+// convert sets `fail`, after which every operation does nothing; running
+// into the end sets `eof`; numbers follow num_get's grammar (an int is
+// [+-]digits, overflow saturates and fails; a double is
+// [+-]digits[.digits][(e|E)[+-]digits] converted by strtod, out of range
+// fails; a bool is an integer 0 or 1, anything else fails and reads true).
+// Parsing from memory instead of through a stream is several times faster on
+// files of millions of lines.
+class Scan {
+public:
+    bool open(const std::string& path) {
+        std::ifstream f(path, std::ios::binary);
+        if (!f) return false;
+        f.seekg(0, std::ios::end);
+        const std::streamoff n = f.tellg();
+        if (n < 0) return false;
+        f.seekg(0, std::ios::beg);
+        s_.resize(static_cast<size_t>(n));
+        if (n > 0 && !f.read(&s_[0], n)) return false;
+        return true;
+    }
+    bool fail() const { return fail_; }
+    bool eof() const { return eof_; }
 
-void expect_word(std::istream& in, const char* word, const std::string& msg) {
+    // ignore(max, delim): up to and including the next delim, or to the end.
+    void ignore_past(char delim) {
+        if (!good()) {
+            fail_ = true;
+            return;
+        }
+        const size_t q = s_.find(delim, p_);
+        if (q == std::string::npos) {
+            p_ = s_.size();
+            eof_ = true;
+        } else {
+            p_ = q + 1;
+        }
+    }
+    // ignore(1)
+    void ignore_one() {
+        if (!good()) {
+            fail_ = true;
+            return;
+        }
+        if (p_ < s_.size()) ++p_;
+        else eof_ = true;
+    }
+    Scan& operator>>(std::string& w) {
+        if (!begin()) return *this;
+        const size_t q0 = p_;
+        while (p_ < s_.size() && !is_space(s_[p_])) ++p_;
+        if (p_ == s_.size()) eof_ = true;
+        w.assign(s_, q0, p_ - q0);
+        return *this;
+    }
+    Scan& operator>>(int& v) {
+        long long x = 0;
+        if (!read_integer(x)) {
+            v = 0;
+            return *this;
+        }
+        if (x > INT_MAX || x < INT_MIN) {
+            v = x > 0 ? INT_MAX : INT_MIN;
+            fail_ = true;
+        } else {
+            v = static_cast<int>(x);
+        }
+        return *this;
+    }
+    Scan& operator>>(bool& v) {
+        long long x = -1;
+        read_integer(x);
+        if (x == 0 || x == 1) {
+            v = x == 1;
+        } else {
+            v = true;
+            fail_ = true;
+        }
+        return *this;
+    }
+    Scan& operator>>(double& v) {
+        if (!begin()) return *this;
+        const size_t q0 = p_;
+        size_t q = p_;
+        const size_t n = s_.size();
+        auto digits = [&]() {
+            while (q < n && s_[q] >= '0' && s_[q] <= '9') ++q;
+        };
+        if (q < n && (s_[q] == '+' || s_[q] == '-')) ++q;
+        digits();
+        if (q < n && s_[q] == '.') {
+            ++q;
+            digits();
+        }
+        if (q < n && (s_[q] == 'e' || s_[q] == 'E')) {
+            ++q;
+            if (q < n && (s_[q] == '+' || s_[q] == '-')) ++q;
+            digits();
+        }
+        p_ = q;
+        if (p_ == n) eof_ = true;
+        char buf[128];
+        std::string big;
+        const char* tok = buf;
+        const size_t len = q - q0;
+        if (len < sizeof buf) {
+            std::memcpy(buf, s_.data() + q0, len);
+            buf[len] = 0;
+        } else {
+            big.assign(s_, q0, len);
+            tok = big.c_str();
+        }
+        char* end = nullptr;
+        errno = 0;
+        const double x = len ? std::strtod(tok, &end) : 0.0;
+        if (len == 0 || end != tok + len) {
+            v = 0.0;
+            fail_ = true;
+        } else if (std::isinf(x)) {
+            v = x > 0 ? std::numeric_limits<double>::max() : -std::numeric_limits<double>::max();
+            fail_ = true;
+        } else {
+            v = x;
+        }
+        return *this;
+    }
+
+private:
+    static bool is_space(char c) {
+        return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r';
+    }
+    bool good() const { return !fail_ && !eof_; }
+    // The sentry of a formatted read: fails when not good, else skips
+    // whitespace; false (fail and eof set) when only whitespace is left.
+    bool begin() {
+        if (!good()) {
+            fail_ = true;
+            return false;
+        }
+        while (p_ < s_.size() && is_space(s_[p_])) ++p_;
+        if (p_ == s_.size()) {
+            eof_ = fail_ = true;
+            return false;
+        }
+        return true;
+    }
+    bool read_integer(long long& x) {
+        if (!begin()) return false;
+        const size_t n = s_.size();
+        size_t q = p_;
+        bool neg = false;
+        if (s_[q] == '+' || s_[q] == '-') {
+            neg = s_[q] == '-';
+            ++q;
+        }
+        const size_t d0 = q;
+        unsigned long long acc = 0;
+        bool over = false;
+        while (q < n && s_[q] >= '0' && s_[q] <= '9') {
+            const unsigned d = static_cast<unsigned>(s_[q] - '0');
+            if (acc > (ULLONG_MAX - d) / 10) over = true;
+            else acc = acc * 10 + d;
+            ++q;
+        }
+        p_ = q;
+        if (p_ == n) eof_ = true;
+        if (q == d0) {
+            x = 0;
+            fail_ = true;
+            return false;
+        }
+        if (over || acc > static_cast<unsigned long long>(LLONG_MAX)) {
+            x = neg ? LLONG_MIN : LLONG_MAX;
+            return true;
+        }
+        x = neg ? -static_cast<long long>(acc) : static_cast<long long>(acc);
+        return true;
+    }
+
+    std::string s_;
+    size_t p_ = 0;
+    bool fail_ = false, eof_ = false;
+};
+
+void expect_word(Scan& in, const char* word, const std::string& msg) {
     std::string temp;
     in >> temp;
     if (temp != word) throw std::runtime_error(msg);
@@ -25,21 +216,21 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
                    std::vector<std::array<double, 3>>& ansatz_node_positions, std::vector<Tri>& triangles,
                    DMat& abar_info, DMat& bbar_info, Stuff& stuff, double& dial_factor_to_start_from, Log& log) {
     log << "Beginning reading of reference data file." << std::endl;
-    std::ifstream in(stuff.ref_data_filepath);
-    if (!in) throw std::runtime_error("Error: Problem opening reference data file.");
-    for (int i = 0; i < 4; ++i) in.ignore(kMax, '\n');
-    in.ignore(kMax, ' ');
+    Scan in;
+    if (!in.open(stuff.ref_data_filepath)) throw std::runtime_error("Error: Problem opening reference data file.");
+    for (int i = 0; i < 4; ++i) in.ignore_past('\n');
+    in.ignore_past(' ');
     stuff.num_nodes = 0;
     in >> stuff.num_nodes;
     if (!(stuff.num_nodes > 0))
         throw std::runtime_error("Error: Problem with (or before) line giving number of nodes in reference data file.");
     nodes.assign(stuff.num_nodes, Node());
     node_positions.resize(stuff.num_nodes, 3);
-    in.ignore(kMax, '\n');
+    in.ignore_past('\n');
     for (int n = 0; n < stuff.num_nodes; ++n) {
         nodes[n].id = n;
         in >> node_positions(n, 0) >> node_positions(n, 1) >> node_positions(n, 2);
-        in.ignore(kMax, '\n');
+        in.ignore_past('\n');
     }
     expect_word(in, "POLYGONS",
                 "Error: Problem with reference data file, at or before 'POLYGONS' line. E.g. may have provided or "
@@ -49,12 +240,12 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
     if (!(stuff.num_tris > 0))
         throw std::runtime_error("Error: Problem with line giving number of triangles in reference data file.");
     triangles.assign(stuff.num_tris, Tri());
-    in.ignore(kMax, '\n');
+    in.ignore_past('\n');
     for (int t = 0; t < stuff.num_tris; ++t) {
         triangles[t].id = t;
-        in.ignore(1);
+        in.ignore_one();
         in >> triangles[t].vertex_ids[0] >> triangles[t].vertex_ids[1] >> triangles[t].vertex_ids[2];
-        in.ignore(kMax, '\n');
+        in.ignore_past('\n');
     }
     bool found_zero = false;
     for (const auto& tri : triangles)
@@ -73,17 +264,17 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
     expect_word(in, "CELL_DATA",
                 "Error: Problem with reference data file, at or before 'CELL_DATA' line. E.g. you may have provided "
                 "or stated wrong number of triangles.");
-    in.ignore(kMax, '\n');
-    in.ignore(kMax, '\n');
+    in.ignore_past('\n');
+    in.ignore_past('\n');
     expect_word(in, "abar_info", "Error: Problem with reference data file, at or before an abar_info line.");
     int ka = 0;
     in >> ka;
     if (ka <= 0) throw std::runtime_error("Error: Problem with reference data file, at or before an abar_info line.");
     abar_info.resize(stuff.num_tris, ka);
-    in.ignore(kMax, '\n');
+    in.ignore_past('\n');
     for (int t = 0; t < stuff.num_tris; ++t) {
         for (int p = 0; p < ka; ++p) in >> abar_info(t, p);
-        in.ignore(kMax, '\n');
+        in.ignore_past('\n');
     }
     expect_word(in, "bbar_info",
                 "Error: Problem with reference data file, at or before a bbar_info line. E.g. you may have provided "
@@ -93,63 +284,62 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
     if (kb <= 0)
         throw std::runtime_error("Error: Problem with reference data file, at or before a bbar_info line.");
     bbar_info.resize(stuff.num_tris, kb);
-    in.ignore(kMax, '\n');
+    in.ignore_past('\n');
     for (int t = 0; t < stuff.num_tris; ++t) {
         for (int p = 0; p < kb; ++p) in >> bbar_info(t, p);
-        in.ignore(kMax, '\n');
+        in.ignore_past('\n');
     }
     expect_word(in, "ref_thicknesses",
                 "Error: Problem with reference data file, at or before a ref_thicknesses line. E.g. you may have "
                 "provided wrong number of bbar_info lines.");
-    in.ignore(kMax, '\n');
+    in.ignore_past('\n');
     if (stuff.ref_thickness_if_uniform > 0)
         log << "Using uniform ref_thickness = " << stuff.ref_thickness_if_uniform << std::endl;
     else
         log << "Using non-uniform ref_thickness from vtk file. " << std::endl;
     for (int t = 0; t < stuff.num_tris; ++t) {
         in >> triangles[t].ref_thickness;
-        in.ignore(kMax, '\n');
+        in.ignore_past('\n');
         if (stuff.ref_thickness_if_uniform > 0) triangles[t].ref_thickness = stuff.ref_thickness_if_uniform;
     }
     expect_word(in, "ref_shear_moduli",
                 "Error: Problem with reference data file, at or before a ref_shear_moduli line. E.g. you may have "
                 "provided wrong number of ref_thicknesses lines.");
-    in.ignore(kMax, '\n');
+    in.ignore_past('\n');
     if (stuff.ref_shear_modulus_if_uniform > 0)
         log << "Using uniform ref_shear_modulus = " << stuff.ref_shear_modulus_if_uniform << std::endl;
     else
         log << "Using non-uniform ref_shear_modulus from vtk file. " << std::endl;
     for (int t = 0; t < stuff.num_tris; ++t) {
         in >> triangles[t].ref_shear_modulus;
-        in.ignore(kMax, '\n');
+        in.ignore_past('\n');
         if (stuff.ref_shear_modulus_if_uniform > 0) triangles[t].ref_shear_modulus = stuff.ref_shear_modulus_if_uniform;
     }
     expect_word(in, "tri_tags", "Error: Problem with reference data file, at or before tri_tags.");
-    in.ignore(kMax, '\n');
-    in.unsetf(std::ios_base::boolalpha);
+    in.ignore_past('\n');
     for (int t = 0; t < stuff.num_tris; ++t) {
         in >> triangles[t].tag;
-        in.ignore(kMax, '\n');
+        in.ignore_past('\n');
     }
     expect_word(in, "POINT_DATA",
                 "Error: Problem with reference data file, at or before 'POINT_DATA'. E.g. you may have provided "
                 "wrong number of ref_thickness values.");
-    in.ignore(kMax, '\n');
-    in.ignore(kMax, '\n');
+    in.ignore_past('\n');
+    in.ignore_past('\n');
     expect_word(in, "constraint_indicators",
                 "Error: Problem with reference data file, at or before constraint_indicators.");
-    in.ignore(kMax, '\n');
+    in.ignore_past('\n');
     for (int n = 0; n < stuff.num_nodes; ++n) {
         in >> nodes[n].is_constrained;
-        in.ignore(kMax, '\n');
+        in.ignore_past('\n');
     }
     expect_word(in, "node_tags", "Error: Problem with reference data file, at or before node_tags.");
-    in.ignore(kMax, '\n');
+    in.ignore_past('\n');
     for (int n = 0; n < stuff.num_nodes; ++n) {
         in >> nodes[n].tag;
-        in.ignore(kMax, '\n');
+        in.ignore_past('\n');
     }
-    if (in.bad() || in.fail())
+    if (in.fail())
         throw std::runtime_error(
             "Error: Unkown problem with reference data file. One of .bad(), .fail() was true - investigate! "
             "E.g. you may not have supplied enough node indicator data in the file, so the file may have reached "
@@ -166,33 +356,33 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
 
     if (stuff.ansatz_file_was_given) {
         log << "Beginning reading of ansatz data file." << std::endl;
-        std::ifstream an(stuff.ansatz_filepath);
-        if (!an) throw std::runtime_error("Error: Problem opening ansatz data file.");
-        an.ignore(kMax, '\n');
-        an.ignore(kMax, ' ');
-        an.ignore(kMax, ' ');
+        Scan an;
+        if (!an.open(stuff.ansatz_filepath)) throw std::runtime_error("Error: Problem opening ansatz data file.");
+        an.ignore_past('\n');
+        an.ignore_past(' ');
+        an.ignore_past(' ');
         dial_factor_to_start_from = -1.0;
         an >> dial_factor_to_start_from;
-        an.ignore(kMax, '\n');
+        an.ignore_past('\n');
         if (!(0 <= dial_factor_to_start_from) || !(dial_factor_to_start_from <= 1))
             throw std::runtime_error(
                 "Error: Problem reading ansatz data file. Remember it must have exactly the correct format.");
-        an.ignore(kMax, '\n');
-        an.ignore(kMax, '\n');
-        an.ignore(kMax, ' ');
+        an.ignore_past('\n');
+        an.ignore_past('\n');
+        an.ignore_past(' ');
         int n_ans = -1;
         an >> n_ans;
         if (n_ans != stuff.num_nodes)
             throw std::runtime_error(
                 "Error: Problem with (or before) line giving number of nodes in ansatz data file. "
                 "E.g. you may have supplied ansatz and ref data files with inconsistent numbers of nodes.");
-        an.ignore(kMax, '\n');
+        an.ignore_past('\n');
         ansatz_node_positions.assign(stuff.num_nodes, {0.0, 0.0, 0.0});
         for (int n = 0; n < stuff.num_nodes; ++n) {
             an >> ansatz_node_positions[n][0] >> ansatz_node_positions[n][1] >> ansatz_node_positions[n][2];
-            an.ignore(kMax, '\n');
+            an.ignore_past('\n');
         }
-        if (an.bad() || an.fail())
+        if (an.fail())
             throw std::runtime_error(
                 "Error: Unkown problem with ansatz data file. One of .bad(), .fail() was true - investigate! "
                 " E.g. you may not have supplied enough ansatz node positions, so the file reached its end "
