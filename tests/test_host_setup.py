@@ -193,3 +193,33 @@ def test_parallel_setup_matches_serial(tmp_path, monkeypatch):
         out.append(m.tables())
     for k in out[0]:
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+def test_ansatz_file_is_read(tmp_path):
+    """An ansatz file in the output format (read_vtk_data.cpp:380-445): its
+    dial factor and node positions become the start of the dynamics; a file
+    with the wrong node count is refused with the reference's message."""
+    from morphoshell_b200 import Model, meshgen
+    mesh, info, bbar = meshgen.workload("disk100")
+    st = tmp_path / "s.txt"
+    st.write_text("\n".join(_settings_text()) + "\n")
+    vtk = tmp_path / "m.vtk"
+    meshgen.write_vtk(str(vtk), "t", mesh.nodes, mesh.tris, info, bbar)
+    N = mesh.nodes.shape[0]
+    rng = np.random.default_rng(3)
+    pos = np.column_stack([mesh.nodes[:, 0], mesh.nodes[:, 1], 0.01 * rng.standard_normal(N)])
+
+    def ansatz_text(n, dial):
+        head = ["# vtk DataFile Version 4.2", "dial_factor = %.14e, stepcount = 1200" % dial, "ASCII",
+                "DATASET POLYDATA", "POINTS %d double" % n]
+        return "\n".join(head + ["%.17g %.17g %.17g" % tuple(p) for p in pos[:n]]) + "\n"
+
+    an = tmp_path / "ansatz.vtk"
+    an.write_text(ansatz_text(N, 0.375))
+    m = Model(str(st), str(vtk), str(an), noise=False)
+    x = m.dofs(1).reshape(3, -1).T
+    assert np.array_equal(x, pos)
+    assert m.scalars.dial_factor_to_start_from == 0.375
+    an.write_text(ansatz_text(N - 1, 0.375))
+    with pytest.raises(RuntimeError, match="number of nodes in ansatz data file"):
+        Model(str(st), str(vtk), str(an), noise=False)
