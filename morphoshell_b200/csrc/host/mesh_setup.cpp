@@ -34,39 +34,6 @@ double vmax(const std::vector<double>& v, size_t* arg = nullptr) {
     return *it;
 }
 
-// Threads for the per-triangle set-up loops: MORPHOSHELL_SETUP_THREADS, else
-// the hardware's; one for small meshes.
-int setup_threads(int n) {
-    if (n < 4096) return 1;
-    int t = (int)std::thread::hardware_concurrency();
-    if (const char* e = std::getenv("MORPHOSHELL_SETUP_THREADS")) t = std::atoi(e);
-    return std::max(1, std::min(t, 128));
-}
-
-// f(begin, end, worker) over [0, n) in contiguous ranges, one per thread.
-// The first exception (of the lowest range) is rethrown after all joined.
-template <typename F>
-void parallel_ranges(int n, int threads, F f) {
-    if (threads <= 1) {
-        f(0, n, 0);
-        return;
-    }
-    std::vector<std::thread> pool;
-    std::vector<std::exception_ptr> errs(threads);
-    const int chunk = (n + threads - 1) / threads;
-    for (int w = 0; w < threads; ++w)
-        pool.emplace_back([&, w]() {
-            try {
-                f(std::min(n, w * chunk), std::min(n, (w + 1) * chunk), w);
-            } catch (...) {
-                errs[w] = std::current_exception();
-            }
-        });
-    for (auto& t : pool) t.join();
-    for (auto& e : errs)
-        if (e) std::rethrow_exception(e);
-}
-
 }  // namespace
 
 // source_files/kahan_sum.cpp:32-49

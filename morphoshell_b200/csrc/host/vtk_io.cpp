@@ -28,21 +28,14 @@ namespace {
 // fails; a bool is an integer 0 or 1, anything else fails and reads true).
 // Parsing from memory instead of through a stream is several times faster on
 // files of millions of lines.
-class Scan {
+class Cursor {
 public:
-    bool open(const std::string& path) {
-        std::ifstream f(path, std::ios::binary);
-        if (!f) return false;
-        f.seekg(0, std::ios::end);
-        const std::streamoff n = f.tellg();
-        if (n < 0) return false;
-        f.seekg(0, std::ios::beg);
-        s_.resize(static_cast<size_t>(n));
-        if (n > 0 && !f.read(&s_[0], n)) return false;
-        return true;
-    }
+    Cursor() = default;
+    // The window [p, n) of d.
+    Cursor(const char* d, size_t n, size_t p) : d_(d), n_(n), p_(p) {}
     bool fail() const { return fail_; }
     bool eof() const { return eof_; }
+    size_t pos() const { return p_; }
 
     // ignore(max, delim): up to and including the next delim, or to the end.
     void ignore_past(char delim) {
@@ -50,12 +43,12 @@ public:
             fail_ = true;
             return;
         }
-        const size_t q = s_.find(delim, p_);
-        if (q == std::string::npos) {
-            p_ = s_.size();
+        const void* q = p_ < n_ ? std::memchr(d_ + p_, delim, n_ - p_) : nullptr;
+        if (!q) {
+            p_ = n_;
             eof_ = true;
         } else {
-            p_ = q + 1;
+            p_ = static_cast<size_t>(static_cast<const char*>(q) - d_) + 1;
         }
     }
     // ignore(1)
@@ -64,18 +57,18 @@ public:
             fail_ = true;
             return;
         }
-        if (p_ < s_.size()) ++p_;
+        if (p_ < n_) ++p_;
         else eof_ = true;
     }
-    Scan& operator>>(std::string& w) {
+    Cursor& operator>>(std::string& w) {
         if (!begin()) return *this;
         const size_t q0 = p_;
-        while (p_ < s_.size() && !is_space(s_[p_])) ++p_;
-        if (p_ == s_.size()) eof_ = true;
-        w.assign(s_, q0, p_ - q0);
+        while (p_ < n_ && !is_space(d_[p_])) ++p_;
+        if (p_ == n_) eof_ = true;
+        w.assign(d_ + q0, p_ - q0);
         return *this;
     }
-    Scan& operator>>(int& v) {
+    Cursor& operator>>(int& v) {
         long long x = 0;
         if (!read_integer(x)) {
             v = 0;
@@ -89,7 +82,7 @@ public:
         }
         return *this;
     }
-    Scan& operator>>(bool& v) {
+    Cursor& operator>>(bool& v) {
         long long x = -1;
         read_integer(x);
         if (x == 0 || x == 1) {
@@ -100,40 +93,38 @@ public:
         }
         return *this;
     }
-    Scan& operator>>(double& v) {
+    Cursor& operator>>(double& v) {
         if (!begin()) return *this;
         const size_t q0 = p_;
         size_t q = p_;
-        const size_t n = s_.size();
         auto digits = [&]() {
-            while (q < n && s_[q] >= '0' && s_[q] <= '9') ++q;
+            while (q < n_ && d_[q] >= '0' && d_[q] <= '9') ++q;
         };
-        if (q < n && (s_[q] == '+' || s_[q] == '-')) ++q;
+        if (q < n_ && (d_[q] == '+' || d_[q] == '-')) ++q;
         digits();
-        if (q < n && s_[q] == '.') {
+        if (q < n_ && d_[q] == '.') {
             ++q;
             digits();
         }
-        if (q < n && (s_[q] == 'e' || s_[q] == 'E')) {
+        if (q < n_ && (d_[q] == 'e' || d_[q] == 'E')) {
             ++q;
-            if (q < n && (s_[q] == '+' || s_[q] == '-')) ++q;
+            if (q < n_ && (d_[q] == '+' || d_[q] == '-')) ++q;
             digits();
         }
         p_ = q;
-        if (p_ == n) eof_ = true;
+        if (p_ == n_) eof_ = true;
         char buf[128];
         std::string big;
         const char* tok = buf;
         const size_t len = q - q0;
         if (len < sizeof buf) {
-            std::memcpy(buf, s_.data() + q0, len);
+            std::memcpy(buf, d_ + q0, len);
             buf[len] = 0;
         } else {
-            big.assign(s_, q0, len);
+            big.assign(d_ + q0, len);
             tok = big.c_str();
         }
         char* end = nullptr;
-        errno = 0;
         const double x = len ? std::strtod(tok, &end) : 0.0;
         if (len == 0 || end != tok + len) {
             v = 0.0;
@@ -147,7 +138,7 @@ public:
         return *this;
     }
 
-private:
+protected:
     static bool is_space(char c) {
         return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r';
     }
@@ -159,8 +150,8 @@ private:
             fail_ = true;
             return false;
         }
-        while (p_ < s_.size() && is_space(s_[p_])) ++p_;
-        if (p_ == s_.size()) {
+        while (p_ < n_ && is_space(d_[p_])) ++p_;
+        if (p_ == n_) {
             eof_ = fail_ = true;
             return false;
         }
@@ -168,24 +159,23 @@ private:
     }
     bool read_integer(long long& x) {
         if (!begin()) return false;
-        const size_t n = s_.size();
         size_t q = p_;
         bool neg = false;
-        if (s_[q] == '+' || s_[q] == '-') {
-            neg = s_[q] == '-';
+        if (d_[q] == '+' || d_[q] == '-') {
+            neg = d_[q] == '-';
             ++q;
         }
         const size_t d0 = q;
         unsigned long long acc = 0;
         bool over = false;
-        while (q < n && s_[q] >= '0' && s_[q] <= '9') {
-            const unsigned d = static_cast<unsigned>(s_[q] - '0');
-            if (acc > (ULLONG_MAX - d) / 10) over = true;
-            else acc = acc * 10 + d;
+        while (q < n_ && d_[q] >= '0' && d_[q] <= '9') {
+            const unsigned dg = static_cast<unsigned>(d_[q] - '0');
+            if (acc > (ULLONG_MAX - dg) / 10) over = true;
+            else acc = acc * 10 + dg;
             ++q;
         }
         p_ = q;
-        if (p_ == n) eof_ = true;
+        if (p_ == n_) eof_ = true;
         if (q == d0) {
             x = 0;
             fail_ = true;
@@ -199,12 +189,68 @@ private:
         return true;
     }
 
-    std::string s_;
-    size_t p_ = 0;
+    const char* d_ = nullptr;
+    size_t n_ = 0, p_ = 0;
     bool fail_ = false, eof_ = false;
 };
 
-void expect_word(Scan& in, const char* word, const std::string& msg) {
+// The whole file with a cursor over it.
+class Scan : public Cursor {
+public:
+    bool open(const std::string& path) {
+        std::ifstream f(path, std::ios::binary);
+        if (!f) return false;
+        f.seekg(0, std::ios::end);
+        const std::streamoff n = f.tellg();
+        if (n < 0) return false;
+        f.seekg(0, std::ios::beg);
+        s_.resize(static_cast<size_t>(n));
+        if (n > 0 && !f.read(&s_[0], n)) return false;
+        d_ = s_.data();
+        n_ = s_.size();
+        p_ = 0;
+        return true;
+    }
+
+    // The next `count` lines, each read by line(cursor, i) with a cursor
+    // limited to that line (without its newline), in parallel; afterwards
+    // the position is past the last line, as after reading each line and
+    // ignore_past('\n').  Returns false, with nothing moved, unless every
+    // line is there and reads without a failure, i.e. unless the stream
+    // reads of those lines would have found the same values on the same
+    // lines; the caller then reads the lines one after another instead.
+    template <typename F>
+    bool lines_in_parallel(int count, F line) {
+        if (!good() || count <= 0) return false;
+        std::vector<size_t> start(static_cast<size_t>(count) + 1);
+        size_t q = p_;
+        for (int i = 0; i < count; ++i) {
+            start[i] = q;
+            const void* nl = q < n_ ? std::memchr(d_ + q, '\n', n_ - q) : nullptr;
+            if (!nl) return false;
+            q = static_cast<size_t>(static_cast<const char*>(nl) - d_) + 1;
+        }
+        start[count] = q;
+        const int threads = setup_threads(count);
+        std::vector<char> ok(threads, 1);
+        parallel_ranges(count, threads, [&](int a, int b, int w) {
+            for (int i = a; i < b && ok[w]; ++i) {
+                Cursor c(d_, start[i + 1] - 1, start[i]);
+                line(c, i);
+                if (c.fail()) ok[w] = 0;
+            }
+        });
+        for (char k : ok)
+            if (!k) return false;
+        p_ = q;
+        return true;
+    }
+
+private:
+    std::string s_;
+};
+
+void expect_word(Cursor& in, const char* word, const std::string& msg) {
     std::string temp;
     in >> temp;
     if (temp != word) throw std::runtime_error(msg);
@@ -227,11 +273,16 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
     nodes.assign(stuff.num_nodes, Node());
     node_positions.resize(stuff.num_nodes, 3);
     in.ignore_past('\n');
-    for (int n = 0; n < stuff.num_nodes; ++n) {
-        nodes[n].id = n;
-        in >> node_positions(n, 0) >> node_positions(n, 1) >> node_positions(n, 2);
-        in.ignore_past('\n');
-    }
+    // The big blocks read their lines in parallel when they are well formed
+    // (Scan::lines_in_parallel), else one after another as the reference does.
+    for (int n = 0; n < stuff.num_nodes; ++n) nodes[n].id = n;
+    if (!in.lines_in_parallel(stuff.num_nodes, [&](Cursor& c, int n) {
+            c >> node_positions(n, 0) >> node_positions(n, 1) >> node_positions(n, 2);
+        }))
+        for (int n = 0; n < stuff.num_nodes; ++n) {
+            in >> node_positions(n, 0) >> node_positions(n, 1) >> node_positions(n, 2);
+            in.ignore_past('\n');
+        }
     expect_word(in, "POLYGONS",
                 "Error: Problem with reference data file, at or before 'POLYGONS' line. E.g. may have provided or "
                 "stated wrong number of nodes.");
@@ -241,12 +292,16 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
         throw std::runtime_error("Error: Problem with line giving number of triangles in reference data file.");
     triangles.assign(stuff.num_tris, Tri());
     in.ignore_past('\n');
-    for (int t = 0; t < stuff.num_tris; ++t) {
-        triangles[t].id = t;
-        in.ignore_one();
-        in >> triangles[t].vertex_ids[0] >> triangles[t].vertex_ids[1] >> triangles[t].vertex_ids[2];
-        in.ignore_past('\n');
-    }
+    for (int t = 0; t < stuff.num_tris; ++t) triangles[t].id = t;
+    if (!in.lines_in_parallel(stuff.num_tris, [&](Cursor& c, int t) {
+            c.ignore_one();
+            c >> triangles[t].vertex_ids[0] >> triangles[t].vertex_ids[1] >> triangles[t].vertex_ids[2];
+        }))
+        for (int t = 0; t < stuff.num_tris; ++t) {
+            in.ignore_one();
+            in >> triangles[t].vertex_ids[0] >> triangles[t].vertex_ids[1] >> triangles[t].vertex_ids[2];
+            in.ignore_past('\n');
+        }
     bool found_zero = false;
     for (const auto& tri : triangles)
         for (int v = 0; v < 3; ++v) found_zero |= (tri.vertex_ids[v] == 0);
@@ -272,10 +327,13 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
     if (ka <= 0) throw std::runtime_error("Error: Problem with reference data file, at or before an abar_info line.");
     abar_info.resize(stuff.num_tris, ka);
     in.ignore_past('\n');
-    for (int t = 0; t < stuff.num_tris; ++t) {
-        for (int p = 0; p < ka; ++p) in >> abar_info(t, p);
-        in.ignore_past('\n');
-    }
+    if (!in.lines_in_parallel(stuff.num_tris, [&](Cursor& c, int t) {
+            for (int p = 0; p < ka; ++p) c >> abar_info(t, p);
+        }))
+        for (int t = 0; t < stuff.num_tris; ++t) {
+            for (int p = 0; p < ka; ++p) in >> abar_info(t, p);
+            in.ignore_past('\n');
+        }
     expect_word(in, "bbar_info",
                 "Error: Problem with reference data file, at or before a bbar_info line. E.g. you may have provided "
                 "wrong number of abar_info lines.");
@@ -285,10 +343,13 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
         throw std::runtime_error("Error: Problem with reference data file, at or before a bbar_info line.");
     bbar_info.resize(stuff.num_tris, kb);
     in.ignore_past('\n');
-    for (int t = 0; t < stuff.num_tris; ++t) {
-        for (int p = 0; p < kb; ++p) in >> bbar_info(t, p);
-        in.ignore_past('\n');
-    }
+    if (!in.lines_in_parallel(stuff.num_tris, [&](Cursor& c, int t) {
+            for (int p = 0; p < kb; ++p) c >> bbar_info(t, p);
+        }))
+        for (int t = 0; t < stuff.num_tris; ++t) {
+            for (int p = 0; p < kb; ++p) in >> bbar_info(t, p);
+            in.ignore_past('\n');
+        }
     expect_word(in, "ref_thicknesses",
                 "Error: Problem with reference data file, at or before a ref_thicknesses line. E.g. you may have "
                 "provided wrong number of bbar_info lines.");
@@ -297,11 +358,13 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
         log << "Using uniform ref_thickness = " << stuff.ref_thickness_if_uniform << std::endl;
     else
         log << "Using non-uniform ref_thickness from vtk file. " << std::endl;
-    for (int t = 0; t < stuff.num_tris; ++t) {
-        in >> triangles[t].ref_thickness;
-        in.ignore_past('\n');
-        if (stuff.ref_thickness_if_uniform > 0) triangles[t].ref_thickness = stuff.ref_thickness_if_uniform;
-    }
+    if (!in.lines_in_parallel(stuff.num_tris, [&](Cursor& c, int t) { c >> triangles[t].ref_thickness; }))
+        for (int t = 0; t < stuff.num_tris; ++t) {
+            in >> triangles[t].ref_thickness;
+            in.ignore_past('\n');
+        }
+    if (stuff.ref_thickness_if_uniform > 0)
+        for (auto& tri : triangles) tri.ref_thickness = stuff.ref_thickness_if_uniform;
     expect_word(in, "ref_shear_moduli",
                 "Error: Problem with reference data file, at or before a ref_shear_moduli line. E.g. you may have "
                 "provided wrong number of ref_thicknesses lines.");
@@ -310,17 +373,20 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
         log << "Using uniform ref_shear_modulus = " << stuff.ref_shear_modulus_if_uniform << std::endl;
     else
         log << "Using non-uniform ref_shear_modulus from vtk file. " << std::endl;
-    for (int t = 0; t < stuff.num_tris; ++t) {
-        in >> triangles[t].ref_shear_modulus;
-        in.ignore_past('\n');
-        if (stuff.ref_shear_modulus_if_uniform > 0) triangles[t].ref_shear_modulus = stuff.ref_shear_modulus_if_uniform;
-    }
+    if (!in.lines_in_parallel(stuff.num_tris, [&](Cursor& c, int t) { c >> triangles[t].ref_shear_modulus; }))
+        for (int t = 0; t < stuff.num_tris; ++t) {
+            in >> triangles[t].ref_shear_modulus;
+            in.ignore_past('\n');
+        }
+    if (stuff.ref_shear_modulus_if_uniform > 0)
+        for (auto& tri : triangles) tri.ref_shear_modulus = stuff.ref_shear_modulus_if_uniform;
     expect_word(in, "tri_tags", "Error: Problem with reference data file, at or before tri_tags.");
     in.ignore_past('\n');
-    for (int t = 0; t < stuff.num_tris; ++t) {
-        in >> triangles[t].tag;
-        in.ignore_past('\n');
-    }
+    if (!in.lines_in_parallel(stuff.num_tris, [&](Cursor& c, int t) { c >> triangles[t].tag; }))
+        for (int t = 0; t < stuff.num_tris; ++t) {
+            in >> triangles[t].tag;
+            in.ignore_past('\n');
+        }
     expect_word(in, "POINT_DATA",
                 "Error: Problem with reference data file, at or before 'POINT_DATA'. E.g. you may have provided "
                 "wrong number of ref_thickness values.");
@@ -329,16 +395,18 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
     expect_word(in, "constraint_indicators",
                 "Error: Problem with reference data file, at or before constraint_indicators.");
     in.ignore_past('\n');
-    for (int n = 0; n < stuff.num_nodes; ++n) {
-        in >> nodes[n].is_constrained;
-        in.ignore_past('\n');
-    }
+    if (!in.lines_in_parallel(stuff.num_nodes, [&](Cursor& c, int n) { c >> nodes[n].is_constrained; }))
+        for (int n = 0; n < stuff.num_nodes; ++n) {
+            in >> nodes[n].is_constrained;
+            in.ignore_past('\n');
+        }
     expect_word(in, "node_tags", "Error: Problem with reference data file, at or before node_tags.");
     in.ignore_past('\n');
-    for (int n = 0; n < stuff.num_nodes; ++n) {
-        in >> nodes[n].tag;
-        in.ignore_past('\n');
-    }
+    if (!in.lines_in_parallel(stuff.num_nodes, [&](Cursor& c, int n) { c >> nodes[n].tag; }))
+        for (int n = 0; n < stuff.num_nodes; ++n) {
+            in >> nodes[n].tag;
+            in.ignore_past('\n');
+        }
     if (in.fail())
         throw std::runtime_error(
             "Error: Unkown problem with reference data file. One of .bad(), .fail() was true - investigate! "
@@ -378,10 +446,13 @@ void read_vtk_data(std::vector<Node>& nodes, DMat& node_positions,
                 "E.g. you may have supplied ansatz and ref data files with inconsistent numbers of nodes.");
         an.ignore_past('\n');
         ansatz_node_positions.assign(stuff.num_nodes, {0.0, 0.0, 0.0});
-        for (int n = 0; n < stuff.num_nodes; ++n) {
-            an >> ansatz_node_positions[n][0] >> ansatz_node_positions[n][1] >> ansatz_node_positions[n][2];
-            an.ignore_past('\n');
-        }
+        if (!an.lines_in_parallel(stuff.num_nodes, [&](Cursor& c, int n) {
+                c >> ansatz_node_positions[n][0] >> ansatz_node_positions[n][1] >> ansatz_node_positions[n][2];
+            }))
+            for (int n = 0; n < stuff.num_nodes; ++n) {
+                an >> ansatz_node_positions[n][0] >> ansatz_node_positions[n][1] >> ansatz_node_positions[n][2];
+                an.ignore_past('\n');
+            }
         if (an.fail())
             throw std::runtime_error(
                 "Error: Unkown problem with ansatz data file. One of .bad(), .fail() was true - investigate! "

@@ -223,3 +223,31 @@ def test_ansatz_file_is_read(tmp_path):
     an.write_text(ansatz_text(N - 1, 0.375))
     with pytest.raises(RuntimeError, match="number of nodes in ansatz data file"):
         Model(str(st), str(vtk), str(an), noise=False)
+
+
+def test_vtk_reader_line_forms(tmp_path):
+    """Blocks are read line by line in parallel only when every line holds
+    its values; other layouts get the stream reader's behaviour: extra
+    values at a line's end are ignored, CRLF line ends read the same, and a
+    line short of a value pulls it from the next line, so the file runs out
+    of step and fails at the next section header."""
+    from morphoshell_b200 import meshgen
+    mesh, info, bbar = meshgen.workload("disk100")
+    good = tmp_path / "g.vtk"
+    meshgen.write_vtk(str(good), "t", mesh.nodes, mesh.tris, info, bbar)
+    text = good.read_text()
+    lines = _settings_text()
+    ref = _load(tmp_path, lines, text).tables()
+
+    def same(m):
+        t = m.tables()
+        return all(np.array_equal(t[k], ref[k]) for k in ref)
+
+    i = text.index("POINTS")
+    first = text.index("\n", i) + 1
+    second = text.index("\n", first)
+    assert same(_load(tmp_path, lines, text[:second] + " 7 8 9" + text[second:]))
+    assert same(_load(tmp_path, lines, text.replace("\n", "\r\n")))
+    short = text[:first] + " ".join(text[first:second].split()[:2]) + text[second:]
+    with pytest.raises(RuntimeError, match="POLYGONS"):
+        _load(tmp_path, lines, short)
