@@ -177,30 +177,34 @@ void calc_mesh_info(std::vector<Node>& nodes, const DMat& P, std::vector<Tri>& t
             "Something is very wrong with the mesh, because the code thinks it has a "
             "negative number of holes! A first thing to check is that all nodes touch at least one tri.");
 
-    // Areas (Tri_Class.cpp:31-36), smallest altitudes, centroids.
-    std::vector<double> areas;
-    for (auto& tri : triangles) {
-        int a = tri.vertex_ids[0], b = tri.vertex_ids[1], c = tri.vertex_ids[2];
-        double s1[3] = {P(b, 0) - P(a, 0), P(b, 1) - P(a, 1), P(b, 2) - P(a, 2)};
-        double s2[3] = {P(c, 0) - P(a, 0), P(c, 1) - P(a, 1), P(c, 2) - P(a, 2)};
-        double cx = 0.5 * (s1[1] * s2[2] - s1[2] * s2[1]);
-        double cy = 0.5 * (s1[2] * s2[0] - s1[0] * s2[2]);
-        double cz = 0.5 * (s1[0] * s2[1] - s1[1] * s2[0]);
-        tri.ref_area = norm3(cx, cy, cz);
-        areas.push_back(tri.ref_area);
-    }
+    // Areas (Tri_Class.cpp:31-36), smallest altitudes, aspect ratios and
+    // centroids per triangle (triangles independent); the sum and the minima
+    // run over them in triangle order afterwards.
+    const int T = static_cast<int>(triangles.size());
+    std::vector<double> areas(T), smallest_alt(T), aspect(T);
+    parallel_ranges(T, nthreads, [&](int t0, int t1, int) {
+        for (int ti = t0; ti < t1; ++ti) {
+            Tri& tri = triangles[ti];
+            const int a = tri.vertex_ids[0], b = tri.vertex_ids[1], c = tri.vertex_ids[2];
+            const double s1[3] = {P(b, 0) - P(a, 0), P(b, 1) - P(a, 1), P(b, 2) - P(a, 2)};
+            const double s2[3] = {P(c, 0) - P(a, 0), P(c, 1) - P(a, 1), P(c, 2) - P(a, 2)};
+            const double cx = 0.5 * (s1[1] * s2[2] - s1[2] * s2[1]);
+            const double cy = 0.5 * (s1[2] * s2[0] - s1[0] * s2[2]);
+            const double cz = 0.5 * (s1[0] * s2[1] - s1[1] * s2[0]);
+            tri.ref_area = norm3(cx, cy, cz);
+            areas[ti] = tri.ref_area;
+            const double l1 = norm3(P(b, 0) - P(a, 0), P(b, 1) - P(a, 1), P(b, 2) - P(a, 2));
+            const double l2 = norm3(P(c, 0) - P(a, 0), P(c, 1) - P(a, 1), P(c, 2) - P(a, 2));
+            const double l3 = norm3(P(c, 0) - P(b, 0), P(c, 1) - P(b, 1), P(c, 2) - P(b, 2));
+            const double alt[3] = {2.0 * tri.ref_area / l1, 2.0 * tri.ref_area / l2, 2.0 * tri.ref_area / l3};
+            const double lo = *std::min_element(alt, alt + 3), hi = *std::max_element(alt, alt + 3);
+            smallest_alt[ti] = lo;
+            aspect[ti] = lo / hi;
+            for (int k = 0; k < 3; ++k)
+                tri.ref_centroid[k] = (P(a, k) + P(b, k) + P(c, k)) / 3.0;
+        }
+    });
     stuff.total_ref_area = kahan_sum(areas);
-    std::vector<double> smallest_alt, aspect;
-    for (const auto& tri : triangles) {
-        int a = tri.vertex_ids[0], b = tri.vertex_ids[1], c = tri.vertex_ids[2];
-        double l1 = norm3(P(b, 0) - P(a, 0), P(b, 1) - P(a, 1), P(b, 2) - P(a, 2));
-        double l2 = norm3(P(c, 0) - P(a, 0), P(c, 1) - P(a, 1), P(c, 2) - P(a, 2));
-        double l3 = norm3(P(c, 0) - P(b, 0), P(c, 1) - P(b, 1), P(c, 2) - P(b, 2));
-        std::vector<double> alt{2.0 * tri.ref_area / l1, 2.0 * tri.ref_area / l2, 2.0 * tri.ref_area / l3};
-        double lo = vmin(alt), hi = vmax(alt);
-        smallest_alt.push_back(lo);
-        aspect.push_back(lo / hi);
-    }
     size_t smallest_tri = 0, worst_tri = 0;
     stuff.approx_min_tri_size = vmin(smallest_alt, &smallest_tri);
     double worst = vmin(aspect, &worst_tri);
@@ -208,9 +212,6 @@ void calc_mesh_info(std::vector<Node>& nodes, const DMat& P, std::vector<Tri>& t
         << std::endl;
     log << "Worst tri aspect ratio = " << worst << " (tri " << worst_tri
         << "). Around 0 is bad, 1 would be perfection." << std::endl;
-    for (auto& tri : triangles)
-        for (int k = 0; k < 3; ++k)
-            tri.ref_centroid[k] = (P(tri.vertex_ids[0], k) + P(tri.vertex_ids[1], k) + P(tri.vertex_ids[2], k)) / 3.0;
 }
 
 
