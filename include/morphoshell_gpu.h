@@ -404,6 +404,20 @@ void* ms_mlp_stream(ms_mlp* h);
 
 #ifdef __cplusplus
 }
+
+#include <stdexcept>
+
+/* C++ callers: the reference's error convention (a std::runtime_error that
+ * main.cpp catches, logs and turns into return -1; main.cpp:448-474).  A guard
+ * trip carries the reference's own message, "implausibly_high_force"
+ * (advance_dynamics.cpp:71); any other failure the handle's last error, or the
+ * status name when there is no handle or no message. */
+inline void ms_check(int rc, const ms_handle* h) {
+    if (rc == MS_OK) return;
+    if (rc == MS_ERR_IMPLAUSIBLE_FORCE) throw std::runtime_error("implausibly_high_force");
+    const char* m = h ? ms_last_error(h) : nullptr;
+    throw std::runtime_error(m && *m ? m : ms_status_string(rc));
+}
 #endif
 
 #endif /* MORPHOSHELL_GPU_H */

@@ -51,3 +51,36 @@ def test_cli_rejects_bad_arguments(tmp_path):
                        text=True)
     assert r.returncode != 0
     assert "settings file" in r.stderr
+
+
+def test_headers_compile_as_c_and_cpp_and_ms_check_throws(tmp_path):
+    """Both headers compile as C11; in C++ the header's ms_check turns a guard
+    trip into the reference's "implausibly_high_force" and other codes into
+    their status names (no handle)."""
+    import shutil
+    import subprocess
+    if not shutil.which("g++") or not shutil.which("gcc"):
+        pytest.skip("no host compiler")
+    from morphoshell_b200 import LIB_PATH
+    inc = os.path.join(ROOT, "include")
+    c = tmp_path / "h.c"
+    c.write_text('#include "morphoshell_gpu.h"\n#include "morphoshell_host.h"\nint main(void) { return 0; }\n')
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Werror", "-fsyntax-only", "-I", inc, str(c)], check=True)
+    cpp = tmp_path / "h.cpp"
+    cpp.write_text(
+        '#include "morphoshell_gpu.h"\n#include <cstdio>\n'
+        "int main() {\n"
+        "  const int codes[2] = {MS_ERR_IMPLAUSIBLE_FORCE, MS_ERR_INVALID_ARGUMENT};\n"
+        "  for (int rc : codes) {\n"
+        '    try { ms_check(rc, nullptr); std::puts("no throw"); }\n'
+        '    catch (const std::runtime_error& e) { std::puts(e.what()); }\n'
+        "  }\n"
+        "  ms_check(MS_OK, nullptr);\n"
+        "  return 0;\n}\n")
+    exe = tmp_path / "h"
+    lib_dir = os.path.dirname(LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I", inc, str(cpp), "-L", lib_dir, "-lmorphoshell",
+                    "-Wl,-rpath," + lib_dir, "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    assert out[0] == "implausibly_high_force"
+    assert out[1] and out[1] != "no throw"
