@@ -251,3 +251,19 @@ def test_vtk_reader_line_forms(tmp_path):
     short = text[:first] + " ".join(text[first:second].split()[:2]) + text[second:]
     with pytest.raises(RuntimeError, match="POLYGONS"):
         _load(tmp_path, lines, short)
+
+
+def test_set_up_from_file_same_with_one_thread_and_many(tmp_path, monkeypatch):
+    """The file's blocks, the mesh bookkeeping and the patch fit run in
+    parallel ranges; the model does not depend on how many threads."""
+    from morphoshell_b200 import Model, meshgen
+    st, vtk = meshgen.write_workload(str(tmp_path), "disk18k")
+    models = []
+    for threads in ("1", "6"):
+        monkeypatch.setenv("MORPHOSHELL_SETUP_THREADS", threads)
+        models.append(Model(st, vtk, noise=False))
+    a, b = (m.tables() for m in models)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(models[0].dofs(0), models[1].dofs(0))
+    assert models[0].scalars.timestep == models[1].scalars.timestep
